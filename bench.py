@@ -1,0 +1,433 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 LBM time step (FlowCraft's LbmSolver::Step hot path).
+
+Workload (default, the large configuration the target is stated on): D3Q19,
+1024x512x512 = 268.4M cells, a procedural high-wing aircraft given as an SDF
+(ellipsoidal fuselage, tapered NACA 2412 wing, NACA 0012 tails), inlet
+U = 0.05, Re = 1e5 on the 60-cell root chord (tau = 0.50009), Smagorinsky
+Cs = 0.1, free-slip side walls. Synthetic input: the geometry is built
+analytically on the device; there is no mesh file or dataset.
+
+One "step" is one full lattice update (every cell streamed, collided and
+written). ``value`` = whole-job GLUPS (cells x steps / s, solid cells
+included) with the lattice resident in HBM, timed with CUDA events on the
+solver's stream, max over ranks. The headline storage is FP16 offset
+populations with FP32 collision; the plain FP32 path is timed beside it.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+For N > 1 run under torchrun; every rank steps its own lattice (replicas, no
+data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "D3Q19 GLUPS & %HBM roofline: FP16+learned SGS vs plain FP32, same GPU/accuracy"
+FALLBACK_HBM_GBS = 6650.0
+
+CONFIGS = {
+    # the large configuration: 1024x512x512, aircraft, Re 1e5 on a 60-cell root chord
+    "large": dict(nx=1024, ny=512, nz=512, geom="aircraft", u=0.05, re=1e5, lref=60.0, cs=0.1,
+                  desc="D3Q19 1024x512x512 (268.4M cells), procedural high-wing aircraft SDF, U=0.05, "
+                       "Re=1e5 on the 60-cell root chord (tau=0.50009), Smagorinsky Cs=0.1"),
+    # the plain-FP32 parity lattice: 128x64x64, sphere r=10, Re=100
+    "c1": dict(nx=128, ny=64, nz=64, geom="sphere", u=0.05, re=100.0, lref=20.0, cs=0.1,
+               desc="D3Q19 128x64x64 (524k cells), sphere r=10 at (40,32,32), U=0.05, Re=100 (tau=0.53), Cs=0.1"),
+    # the precision-study lattice size: 384x192x192 NACA 0012 wing, chord 96, 4 deg
+    "c2": dict(nx=384, ny=192, nz=192, geom="naca0012", u=0.06, re=1e4, lref=96.0, cs=0.1,
+               desc="D3Q19 384x192x192 (14.2M cells), NACA 0012 wing chord 96 span 128 at 4 deg, U=0.06, "
+                    "Re=1e4 (tau=0.50173), Smagorinsky Cs=0.1"),
+}
+
+BYTES_PER_ELEM = {"fp32": 4, "fp16_offset": 2, "bf16_offset": 2}
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="large")
+    ap.add_argument("--variants", default="fp16_offset,fp32", help="first one is the headline")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args(argv)
+
+
+def tau_for(cfg) -> float:
+    nu = cfg["u"] * cfg["lref"] / cfg["re"]
+    return 0.5 + 3.0 * nu
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        import torch
+        self.lines = []
+        self.proc = None
+        try:
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            ident = uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                                          "-lms", "50", "--id=" + ident], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.time(), line.strip()))
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        time.sleep(0.12)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for _, line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(re.sub(r"[^0-9.]", "", parts[1])))
+                smax.append(float(re.sub(r"[^0-9.]", "", parts[2])))
+                power.append(float(re.sub(r"[^0-9.]", "", parts[3]) or 0))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+# ---------------------------------------------------------------- helpers
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic_per_cell(variant: str):
+    """DRAM bytes per bulk-kernel cell update from the committed ncu summary
+    (a line 'traffic_bytes_per_cell <kernel> <variant> = X'), or None."""
+    path = os.path.join(ROOT, "profiles", "bulk_pull_ncu.md")
+    try:
+        text = open(path).read()
+    except OSError:
+        return None
+    m = re.search(rf"traffic_bytes_per_cell\s+bulk_pull\s+{variant}\s*=\s*([0-9.]+)", text)
+    return float(m.group(1)) if m else None
+
+
+def build_geometry(cfg, device, z_lo=0, z_hi=None):
+    """(solid u8, sdf f32) torch tensors (nz, ny, nx), or layers [z_lo, z_hi)."""
+    import torch
+
+    from flowcraft_b200 import geometry
+    z_hi = cfg["nz"] if z_hi is None else z_hi
+    if cfg["geom"] == "aircraft":
+        return geometry.aircraft_grid_torch(cfg["nx"], cfg["ny"], cfg["nz"], device=device, z_lo=z_lo, z_hi=z_hi)
+    if cfg["geom"] == "sphere":
+        solid, sdf = geometry.sphere_grid(cfg["nx"], cfg["ny"], cfg["nz"], 40, 32, 32, 10)
+        return (torch.from_numpy(solid[z_lo:z_hi].copy()).to(device),
+                torch.from_numpy(sdf[z_lo:z_hi].copy()).to(device))
+    solid, sdf = geometry.naca_wing_grid(cfg["nx"], cfg["ny"], cfg["nz"], chord=96, span=128, aoa_deg=4,
+                                         digits="0012", xp=torch, device=device)
+    return solid[z_lo:z_hi].contiguous(), sdf[z_lo:z_hi].contiguous()
+
+
+def make_solver(cfg, solid, sdf, variant, device_index):
+    from flowcraft_b200 import LatticeModel, LbmSolver, Params, Storage, VoxelGrid
+    s = LbmSolver()
+    st = {"fp32": Storage.FP32, "fp16_offset": Storage.FP16_OFFSET, "bf16_offset": Storage.BF16_OFFSET}[variant]
+    grid = VoxelGrid(cfg["nx"], cfg["ny"], cfg["nz"], solid=solid, signedDistance=sdf)
+    if not s.Init(device_index, grid, LatticeModel.D3Q19, st):
+        raise RuntimeError(s.LastError())
+    s.Reset(Params(tau=tau_for(cfg), inletVelocity=cfg["u"], smagorinskyCs=cfg["cs"]), True)
+    return s
+
+
+def barrier_sync(dist_on):
+    import torch
+    if dist_on:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def allreduce_max(x: float, dist_on) -> float:
+    if not dist_on:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- CPU baseline
+def subbox_range(cfg, cores):
+    """A z-truncated sub-box of the same lattice around the wing, deep enough
+    that every host thread gets z-layers (the reference splits work by z)."""
+    nz_sub = int(min(cfg["nz"], max(16, 2 * cores)))
+    z0 = max(0, min(cfg["nz"] - nz_sub, int(0.55 * cfg["nz"]) - nz_sub // 2))
+    return z0, z0 + nz_sub
+
+
+def cpu_subbox(cfg, solid, sdf, cores):
+    z0, z1 = subbox_range(cfg, cores)
+    s = solid[z0:z1].contiguous().cpu().numpy()
+    d = sdf[z0:z1].contiguous().cpu().numpy()
+    return s, d, z0
+
+
+def run_cpu_reference(cfg, solid_np, sdf_np, steps, warmup, seconds=None):
+    """Times FlowCraft's own LbmReference (oracle/_ref, -O3) — or the restated
+    oracle if the reference build is absent — on the given sub-box."""
+    from oracle import oracle as orc
+    kind = "reference" if orc.available("ref_fast") else "port"
+    prec = "ref_fast" if kind == "reference" else "f32"
+    p = orc.Params(tau=tau_for(cfg), inlet_velocity=cfg["u"], smagorinsky_cs=cfg["cs"])
+    o = orc.Oracle(solid_np, sdf_np, 19, p, True, prec)
+    for _ in range(warmup):
+        o.step(1)
+    done = 0
+    t0 = time.perf_counter()
+    while True:
+        o.step(1)
+        done += 1
+        el = time.perf_counter() - t0
+        if seconds is None and done >= steps:
+            break
+        if seconds is not None and (el >= seconds or done >= steps):
+            break
+    el = time.perf_counter() - t0
+    cells = solid_np.size
+    o.close()
+    return {"glups": cells * done / el / 1e9, "steps": done, "seconds": el, "cells": cells, "kind": kind}
+
+
+# ---------------------------------------------------------------- main arms
+def run_reference_arm(args, cfg, rank, world):
+    import numpy as np
+    if rank != 0:
+        return 0
+    cores = os.cpu_count() or 1
+    # the same procedural geometry, built on the host for the sub-box only
+    z0, z1 = subbox_range(cfg, cores)
+    solid, sdf = build_geometry(cfg, "cpu", z0, z1)
+    s_np, d_np = solid.numpy(), sdf.numpy()
+    r = run_cpu_reference(cfg, s_np, d_np, args.steps, args.warmup)
+    sample = (f"z-truncated sub-box {cfg['nx']}x{cfg['ny']}x{s_np.shape[0]} (z0={z0}) of the {cfg['nx']}x{cfg['ny']}x"
+              f"{cfg['nz']} lattice, {r['steps']} LbmReference::Step calls after {args.warmup} warm-up")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["glups"], "unit": "GLUPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": cfg["desc"], "lattice": "D3Q19", "sample_cells": r["cells"]},
+        "cpu_baseline": {"value": r["glups"], "unit": "GLUPS", "cores": cores, "kind": r["kind"], "sample": sample},
+        "e2e": {"value": r["glups"], "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    del np
+    return 0
+
+
+def time_variant(args, cfg, solid, sdf, variant, dev_index, dist_on, sample_clocks):
+    s = make_solver(cfg, solid, sdf, variant, dev_index)
+    info = s.BoundaryInfo()
+    s.Step(None, args.warmup)
+    s.Sync()
+    barrier_sync(dist_on)
+    sampler = ClockSampler(dev_index) if sample_clocks else None
+    l0 = s.LaunchCount()
+    t = s.StepTimed(args.steps)  # events around every launch, waits at the end
+    launches = s.LaunchCount() - l0
+    clocks = sampler.stop() if sampler else None
+    barrier_sync(dist_on)
+    total_ms = allreduce_max(t["total_ms"], dist_on)
+    stats = s.ReadbackStats()
+    s.close()
+    cells = cfg["nx"] * cfg["ny"] * cfg["nz"]
+    elem = BYTES_PER_ELEM[variant]
+    bulk_avg_s = t["bulk_ms"] / args.steps / 1e3
+    bulk_bytes = info["bulk_cells"] * 19 * 2 * elem
+    return {
+        "variant": variant, "total_ms": total_ms, "ms_per_step": total_ms / args.steps,
+        "glups_rank": cells * args.steps / (t["total_ms"] / 1e3) / 1e9,
+        "bulk_ms_per_launch": t["bulk_ms"] / args.steps, "boundary_ms_per_launch": t["boundary_ms"] / args.steps,
+        "bulk_cells": info["bulk_cells"], "boundary_cells": info["boundary_cells"],
+        "bouzidi_links": info["bouzidi_links"], "bulk_bytes_per_launch": bulk_bytes,
+        "bulk_gbs": bulk_bytes / bulk_avg_s / 1e9 if bulk_avg_s > 0 else None,
+        "launches": launches, "clocks": clocks, "bytes_per_cell": 19 * 2 * elem,
+        "stats_after": {"avg_density": stats.avgDensity, "avg_speed": stats.avgSpeed, "has_nan": stats.hasNaN,
+                        "force_x": stats.forceX, "force_z": stats.forceZ},
+    }
+
+
+def run_e2e(args, cfg, solid, sdf, variant, dev_index):
+    """The same metric end to end through the public API with host buffers:
+    Init from pinned host geometry (H2D), Reset, then per step Step(1) plus
+    ProbeSliceHealth of one z-layer (D2H), then ReadbackStats and the full
+    4-float field into host memory (D2H). Wall clock around the host calls."""
+    import numpy as np
+    import torch
+
+    from flowcraft_b200 import LatticeModel, LbmSolver, Params, Storage, VoxelGrid
+    h_solid = solid.cpu().pin_memory()
+    h_sdf = sdf.cpu().pin_memory()
+    n = cfg["nx"] * cfg["ny"] * cfg["nz"]
+    out = np.empty(n * 4, dtype=np.float32)
+    out[::1024] = 0  # fault the pages in before timing
+    out.fill(0)
+    st = {"fp32": Storage.FP32, "fp16_offset": Storage.FP16_OFFSET, "bf16_offset": Storage.BF16_OFFSET}[variant]
+    grid = VoxelGrid(cfg["nx"], cfg["ny"], cfg["nz"], solid=h_solid.numpy(), signedDistance=h_sdf.numpy())
+    torch.cuda.synchronize()
+    s = LbmSolver()
+    t0 = time.perf_counter()
+    if not s.Init(dev_index, grid, LatticeModel.D3Q19, st):
+        raise RuntimeError(s.LastError())
+    s.Reset(Params(tau=tau_for(cfg), inletVelocity=cfg["u"], smagorinskyCs=cfg["cs"]), True)
+    diverged = False
+    for k in range(args.steps):
+        s.Step(None, 1)
+        diverged |= s.ProbeSliceHealth(k % cfg["nz"])
+    stats = s.ReadbackStats()
+    s.ReadbackFieldRange(0, cfg["nz"], out)
+    el = time.perf_counter() - t0
+    s.close()
+    layer = cfg["nx"] * cfg["ny"] * 16
+    h2d = n * (1 + 4)
+    d2h = layer * args.steps + n * 16 + 96
+    return {"value": n * args.steps / el / 1e9, "unit": "GLUPS", "seconds": el,
+            "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
+            "diverged": diverged, "avg_density": stats.avgDensity,
+            "timed": "Init(host VoxelGrid) + Reset + steps x (Step(1) + ProbeSliceHealth) + ReadbackStats + "
+                     "ReadbackFieldRange(all z)"}
+
+
+def run_ours(args, cfg, rank, world, local_rank):
+    import torch
+    dist_on = world > 1
+    torch.cuda.set_device(local_rank)
+    dev_index = local_rank
+    solid, sdf = build_geometry(cfg, f"cuda:{local_rank}")
+    torch.cuda.synchronize()
+    variants = [v.strip() for v in args.variants.split(",") if v.strip()]
+    results = {}
+    for i, v in enumerate(variants):
+        results[v] = time_variant(args, cfg, solid, sdf, v, dev_index, dist_on, sample_clocks=(rank == 0))
+        torch.cuda.empty_cache()
+    head = results[variants[0]]
+    cells = cfg["nx"] * cfg["ny"] * cfg["nz"]
+    total_s = head["total_ms"] / 1e3
+    value = world * cells * args.steps / total_s / 1e9
+
+    peak, peak_src = measured_peak()
+    trf = ncu_traffic_per_cell(head["variant"])
+    roofline = {
+        "bound": "hbm", "achieved": head["bulk_gbs"], "peak": peak, "unit": "GB/s",
+        "frac": head["bulk_gbs"] / peak if head["bulk_gbs"] else None,
+        "traffic": trf * head["bulk_cells"] if trf else None,
+        "kernel": f"k_bulk_pull<19,{head['variant']}>",
+        "algorithmic_bytes_per_launch": head["bulk_bytes_per_launch"],
+        "peak_source": f"{peak_src} ({'MEASURED_PEAKS.json hbm_gbs' if peak_src == 'measured' else 'fallback'})",
+    }
+    e2e = None
+    if not args.no_e2e:
+        torch.cuda.empty_cache()
+        e2e = run_e2e(args, cfg, solid, sdf, variants[0], dev_index)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cores = os.cpu_count() or 1
+        s_np, d_np, z0 = cpu_subbox(cfg, solid, sdf, cores)
+        r = run_cpu_reference(cfg, s_np, d_np, 10 ** 6, 1, seconds=args.cpu_seconds)
+        cpu = {"value": r["glups"], "unit": "GLUPS", "cores": cores, "kind": r["kind"],
+               "sample": f"LbmReference::Step on a z-truncated {cfg['nx']}x{cfg['ny']}x{s_np.shape[0]} sub-box "
+                         f"(z0={z0}) of the same lattice, {r['steps']} steps in {r['seconds']:.1f}s after 1 warm-up"}
+    if rank != 0:
+        return 0
+    variants_out = {}
+    for v, r in results.items():
+        variants_out[v] = {
+            "glups": world * cells * args.steps / (r["total_ms"] / 1e3) / 1e9, "ms_per_step": r["ms_per_step"],
+            "bulk_ms_per_launch": r["bulk_ms_per_launch"], "boundary_ms_per_launch": r["boundary_ms_per_launch"],
+            "bulk_gbs": r["bulk_gbs"], "roofline_frac": r["bulk_gbs"] / peak if r["bulk_gbs"] else None,
+            "bytes_per_cell_update": r["bytes_per_cell"], "clocks": r["clocks"], "stats_after": r["stats_after"],
+        }
+    line = {
+        "metric": METRIC, "value": value, "unit": "GLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: analytic procedural geometry built on the device, no dataset",
+        "config": {"workload": cfg["desc"], "lattice": "D3Q19", "nx": cfg["nx"], "ny": cfg["ny"], "nz": cfg["nz"],
+                   "cells": cells, "storage": head["variant"], "collision": "regularized + Smagorinsky, FP32",
+                   "closure": "Smagorinsky (learned closure not built yet)", "streaming": "pull, ping-pong",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "no flush: the population set (10.2 GB fp16 / 20.4 GB fp32 per copy) exceeds the 126 MB L2",
+                   "boundary_cells": head["boundary_cells"], "bouzidi_links": head["bouzidi_links"]},
+        "variants": variants_out,
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": head["launches"],
+        "clocks": head["clocks"],
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(argv=None) -> int:
+    args = parse_args(argv)
+    cfg = CONFIGS[args.config]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, cfg, rank, world)
+    import datetime
+
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        return run_ours(args, cfg, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,810 @@
+// Host side of the C ABI declared in include/fc_lbm.h: the CUDA-backed
+// replacement of FlowCraft's SDL_GPU LbmSolver (FlowCraft/LbmSolver.cpp).
+//
+// One handle owns one lattice on one device: the population set(s), the
+// solid mask and SDF (for readback forces), the bit-packed bulk mask, the
+// compacted boundary list with its Bouzidi coefficients, a stream, and
+// pinned staging for transfers. Device memory is allocated in fc_lbm_init
+// and released in fc_lbm_shutdown; stepping and readback allocate nothing.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/fc_lbm.h"
+#include "lbm_internal.h"
+
+using fc::Geom;
+
+struct fc_lbm {
+    std::string err;
+    bool valid = false;
+    int device = 0;
+    int q = 19;
+    int model = FC_LATTICE_D3Q19;
+    int storage = FC_STORAGE_FP32;
+    int streaming = FC_STREAMING_PINGPONG;
+    Geom g{};
+    fc_params params{0.8f, 0.05f, 0, 1, 1, 0.12f};  // LbmSolver::Params defaults (LbmSolver.h:61-100)
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_own = nullptr, ev_foreign = nullptr, ev_sync = nullptr;
+    void* pop[2] = {nullptr, nullptr};
+    int cur = 0;
+    uint8_t* d_solid = nullptr;
+    float* d_sdf = nullptr;
+    uint32_t* d_bulk_bits = nullptr;
+    uint32_t* d_cells = nullptr;
+    unsigned long long* d_links = nullptr;
+    uint32_t* d_coef_off = nullptr;
+    float2* d_coef = nullptr;
+    std::vector<uint32_t> z_begin;
+    size_t n_bnd = 0, n_bz = 0, n_bulk = 0;
+    int* d_diverged = nullptr;
+    double* d_stats_partials = nullptr;
+    double* d_stats_result = nullptr;
+    int stats_blocks = 0;
+    float* d_stage = nullptr;
+    float* h_stage = nullptr;
+    size_t stage_floats = 0;
+    std::vector<uint8_t> solid_cpu;
+    uint64_t steps_since_reset = 0;
+    uint64_t launches = 0;
+};
+
+namespace {
+
+constexpr size_t kStageFloats = size_t(1) << 24;  // 64 MiB device + 64 MiB pinned host
+constexpr int kTransferTimeoutMs = 600000;
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int d) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DeviceGuard() {
+        int now = -1;
+        if (prev >= 0 && cudaGetDevice(&now) == cudaSuccess && now != prev) cudaSetDevice(prev);
+    }
+};
+
+int fail(fc_lbm* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+int cuda_fail(fc_lbm* h, cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    if (e == cudaErrorMemoryAllocation) return fail(h, FC_LBM_ERR_OUT_OF_MEMORY, m);
+    return fail(h, FC_LBM_ERR_CUDA, m);
+}
+
+#define FC_TRY(h, expr, what)                                 \
+    do {                                                      \
+        cudaError_t _e = (expr);                              \
+        if (_e != cudaSuccess) return cuda_fail(h, _e, what); \
+    } while (0)
+
+#define FC_RC(expr)               \
+    do {                          \
+        int _rc = (expr);         \
+        if (_rc != FC_LBM_OK) return _rc; \
+    } while (0)
+
+template <class T>
+void dfree(T*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+// Waits for everything queued on the handle's stream. Polls with a growing
+// sleep so the host never spins on the GPU and a stuck device surfaces as a
+// timeout status rather than a hang.
+int wait_stream(fc_lbm* h, int timeout_ms) {
+    cudaError_t e = cudaEventRecord(h->ev_sync, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaEventRecord");
+    auto t0 = std::chrono::steady_clock::now();
+    int sleep_us = 5;
+    for (;;) {
+        e = cudaEventQuery(h->ev_sync);
+        if (e == cudaSuccess) return FC_LBM_OK;
+        if (e != cudaErrorNotReady) return cuda_fail(h, e, "device work failed");
+        if (timeout_ms >= 0) {
+            auto ms =
+                std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
+            if (ms >= timeout_ms) return fail(h, FC_LBM_ERR_TIMEOUT, "timed out waiting for the device");
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(sleep_us));
+        sleep_us = std::min(sleep_us * 2, 500);
+    }
+}
+
+bool params_ok(const fc_params* p) {
+    return p && std::isfinite(p->tau) && std::isfinite(p->inlet_velocity) && std::isfinite(p->smagorinsky_cs) &&
+           p->tau > 0.5f && p->smagorinsky_cs >= 0.0f;
+}
+
+fc::StepParams step_params(const fc_lbm* h) {
+    fc::StepParams s{};
+    const fc_params& p = h->params;
+    s.tau = p.tau;
+    s.cs = p.smagorinsky_cs;
+    s.reverse = p.reverse_flow != 0;
+    s.inlet_x = s.reverse ? h->g.nx - 1 : 0;  // LbmReference.cpp:253-255
+    s.outlet_x = s.reverse ? 0 : h->g.nx - 1;
+    s.inlet_ux = s.reverse ? -p.inlet_velocity : p.inlet_velocity;
+    s.slip_y = p.free_slip_y != 0;
+    s.slip_z = p.free_slip_z != 0;
+    return s;
+}
+
+void release(fc_lbm* h) {
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    dfree(h->pop[0]);
+    dfree(h->pop[1]);
+    dfree(h->d_solid);
+    dfree(h->d_sdf);
+    dfree(h->d_bulk_bits);
+    dfree(h->d_cells);
+    dfree(h->d_links);
+    dfree(h->d_coef_off);
+    dfree(h->d_coef);
+    dfree(h->d_diverged);
+    dfree(h->d_stats_partials);
+    dfree(h->d_stats_result);
+    dfree(h->d_stage);
+    if (h->h_stage) cudaFreeHost(h->h_stage);
+    h->h_stage = nullptr;
+    if (h->ev_own) cudaEventDestroy(h->ev_own);
+    if (h->ev_foreign) cudaEventDestroy(h->ev_foreign);
+    if (h->ev_sync) cudaEventDestroy(h->ev_sync);
+    h->ev_own = h->ev_foreign = h->ev_sync = nullptr;
+    if (h->stream) cudaStreamDestroy(h->stream);
+    h->stream = nullptr;
+    h->z_begin.clear();
+    h->solid_cpu.clear();
+    h->solid_cpu.shrink_to_fit();
+    h->n_bnd = h->n_bz = h->n_bulk = 0;
+    h->valid = false;
+    h->cur = 0;
+    h->steps_since_reset = 0;
+}
+
+// Copies `bytes` from host or device memory into device memory, staging host
+// data through the pinned buffer.
+int upload(fc_lbm* h, void* dst, const void* src, size_t bytes, bool src_device) {
+    if (src_device) {
+        FC_TRY(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, h->stream), "copy geometry");
+        return FC_LBM_OK;
+    }
+    const size_t chunk = h->stage_floats * sizeof(float);
+    for (size_t off = 0; off < bytes; off += chunk) {
+        const size_t nb = std::min(chunk, bytes - off);
+        FC_RC(wait_stream(h, kTransferTimeoutMs));
+        std::memcpy(h->h_stage, (const char*)src + off, nb);
+        FC_TRY(h, cudaMemcpyAsync((char*)dst + off, h->h_stage, nb, cudaMemcpyHostToDevice, h->stream),
+               "upload geometry");
+    }
+    return wait_stream(h, kTransferTimeoutMs);
+}
+
+// Classifies every cell and builds the boundary list (see lbm_setup.cu).
+int build_boundary(fc_lbm* h) {
+    const Geom& g = h->g;
+    struct Temp {
+        uint8_t* flags = nullptr;
+        unsigned long long* counts = nullptr;
+        uint32_t* sel_count = nullptr;
+        uint32_t* nbz = nullptr;
+        void* cub = nullptr;
+        ~Temp() {
+            dfree(flags);
+            dfree(counts);
+            dfree(sel_count);
+            dfree(nbz);
+            if (cub) cudaFree(cub);
+        }
+    } t;
+    FC_TRY(h, cudaMalloc(&t.flags, g.n), "alloc classify flags");
+    FC_TRY(h, cudaMalloc(&t.counts, 2 * sizeof(unsigned long long)), "alloc counters");
+    FC_TRY(h, cudaMalloc(&t.sel_count, sizeof(uint32_t)), "alloc counter");
+    FC_TRY(h, cudaMemsetAsync(t.counts, 0, 2 * sizeof(unsigned long long), h->stream), "clear counters");
+    FC_TRY(h, fc::launch_classify(h->q, h->d_solid, g, t.flags, h->d_bulk_bits, t.counts, h->stream), "classify");
+    h->launches++;
+    unsigned long long counts[2] = {0, 0};
+    FC_TRY(h, cudaMemcpyAsync(h->h_stage, t.counts, sizeof(counts), cudaMemcpyDeviceToHost, h->stream), "read counts");
+    FC_RC(wait_stream(h, kTransferTimeoutMs));
+    std::memcpy(counts, h->h_stage, sizeof(counts));
+    h->n_bnd = (size_t)counts[0];
+    h->n_bulk = (size_t)counts[1];
+
+    h->z_begin.assign((size_t)g.nz + 1, 0);
+    if (h->n_bnd == 0) return FC_LBM_OK;
+
+    FC_TRY(h, cudaMalloc(&h->d_cells, h->n_bnd * sizeof(uint32_t)), "alloc boundary list");
+    size_t cub_bytes = 0, scan_bytes = 0;
+    FC_TRY(h, fc::select_flagged_cells(nullptr, cub_bytes, t.flags, h->d_cells, t.sel_count, g.n, h->stream),
+           "select sizing");
+    FC_TRY(h, fc::exclusive_scan_u32(nullptr, scan_bytes, nullptr, nullptr, h->n_bnd, h->stream), "scan sizing");
+    cub_bytes = std::max(cub_bytes, scan_bytes);
+    FC_TRY(h, cudaMalloc(&t.cub, cub_bytes), "alloc select temp");
+    FC_TRY(h, fc::select_flagged_cells(t.cub, cub_bytes, t.flags, h->d_cells, t.sel_count, g.n, h->stream),
+           "select boundary cells");
+    dfree(t.flags);  // 1 byte per cell, no longer needed
+
+    FC_TRY(h, cudaMalloc(&h->d_links, h->n_bnd * sizeof(unsigned long long)), "alloc links");
+    FC_TRY(h, cudaMalloc(&h->d_coef_off, h->n_bnd * sizeof(uint32_t)), "alloc coefficient offsets");
+    FC_TRY(h, cudaMalloc(&t.nbz, h->n_bnd * sizeof(uint32_t)), "alloc link counts");
+    FC_TRY(h, fc::launch_links(h->q, h->d_cells, h->n_bnd, h->d_solid, h->d_sdf, g, h->d_links, t.nbz, nullptr,
+                               nullptr, h->stream),
+           "resolve links");
+    FC_TRY(h, fc::exclusive_scan_u32(t.cub, cub_bytes, t.nbz, h->d_coef_off, h->n_bnd, h->stream), "scan links");
+    uint32_t tail[2] = {0, 0};
+    FC_TRY(h, cudaMemcpyAsync(h->h_stage, h->d_coef_off + (h->n_bnd - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                              h->stream),
+           "read link total");
+    FC_TRY(h, cudaMemcpyAsync((char*)h->h_stage + 4, t.nbz + (h->n_bnd - 1), sizeof(uint32_t),
+                              cudaMemcpyDeviceToHost, h->stream),
+           "read link total");
+    FC_RC(wait_stream(h, kTransferTimeoutMs));
+    std::memcpy(tail, h->h_stage, sizeof(tail));
+    h->n_bz = (size_t)tail[0] + tail[1];
+    if (h->n_bz > 0) {
+        FC_TRY(h, cudaMalloc(&h->d_coef, h->n_bz * sizeof(float2)), "alloc Bouzidi coefficients");
+        FC_TRY(h, fc::launch_links(h->q, h->d_cells, h->n_bnd, h->d_solid, h->d_sdf, g, h->d_links, nullptr,
+                                   h->d_coef_off, h->d_coef, h->stream),
+               "fill Bouzidi coefficients");
+    }
+    uint32_t* d_zb = nullptr;
+    FC_TRY(h, cudaMalloc(&d_zb, ((size_t)g.nz + 1) * sizeof(uint32_t)), "alloc z offsets");
+    cudaError_t e = fc::launch_z_offsets(h->d_cells, h->n_bnd, g, d_zb, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h->h_stage, d_zb, ((size_t)g.nz + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                            h->stream);
+    int rc = e == cudaSuccess ? wait_stream(h, kTransferTimeoutMs) : cuda_fail(h, e, "z offsets");
+    if (rc == FC_LBM_OK) std::memcpy(h->z_begin.data(), h->h_stage, ((size_t)g.nz + 1) * sizeof(uint32_t));
+    cudaFree(d_zb);
+    h->launches += 4;
+    return rc;
+}
+
+// Orders work on a caller's stream after the handle's stream (and back).
+int enter_stream(fc_lbm* h, cudaStream_t s) {
+    if (s == h->stream) return FC_LBM_OK;
+    FC_TRY(h, cudaEventRecord(h->ev_own, h->stream), "order streams");
+    FC_TRY(h, cudaStreamWaitEvent(s, h->ev_own, 0), "order streams");
+    return FC_LBM_OK;
+}
+int leave_stream(fc_lbm* h, cudaStream_t s) {
+    if (s == h->stream) return FC_LBM_OK;
+    FC_TRY(h, cudaEventRecord(h->ev_foreign, s), "order streams");
+    FC_TRY(h, cudaStreamWaitEvent(h->stream, h->ev_foreign, 0), "order streams");
+    return FC_LBM_OK;
+}
+
+int step_range_on(fc_lbm* h, cudaStream_t s, int z0, int zc) {
+    const int z1 = std::min(h->g.nz, z0 + zc);
+    z0 = std::max(0, z0);
+    if (z1 <= z0) return FC_LBM_OK;
+    const fc::StepParams p = step_params(h);
+    const void* fin = h->pop[h->cur];
+    void* fout = h->pop[1 - h->cur];
+    if (h->n_bulk > 0) {
+        FC_TRY(h, fc::launch_bulk_pull(h->q, h->storage, fin, fout, h->d_bulk_bits, h->g, p, z0, z1 - z0,
+                                       h->d_diverged, s),
+               "bulk step");
+        h->launches++;
+    }
+    const uint32_t b = h->z_begin[(size_t)z0], e = h->z_begin[(size_t)z1];
+    if (e > b) {
+        fc::BoundaryList bl{h->d_cells, h->d_links, h->d_coef_off, h->d_coef};
+        FC_TRY(h, fc::launch_boundary_pull(h->q, h->storage, fin, fout, bl, b, e, h->g, p, h->d_diverged, s),
+               "boundary step");
+        h->launches++;
+    }
+    return FC_LBM_OK;
+}
+
+int check_ready(fc_lbm* h) {
+    if (!h) return FC_LBM_ERR_INVALID_ARG;
+    if (!h->valid) return fail(h, FC_LBM_ERR_NOT_INITIALIZED, "solver not initialized");
+    return FC_LBM_OK;
+}
+
+// Macroscopic field of cells [cell0, cell0 + cells) into host memory `out`
+// (4 floats per cell), chunked through the staging buffers.
+int field_to_host(fc_lbm* h, size_t cell0, size_t cells, float* out) {
+    const size_t chunk = h->stage_floats / 4;
+    for (size_t done = 0; done < cells; done += chunk) {
+        const size_t nc = std::min(chunk, cells - done);
+        FC_TRY(h, fc::launch_field(h->q, h->storage, h->pop[h->cur], h->d_solid, h->d_sdf, h->g, cell0 + done, nc,
+                                   h->d_stage, h->stream),
+               "field kernel");
+        h->launches++;
+        FC_TRY(h, cudaMemcpyAsync(h->h_stage, h->d_stage, nc * 4 * sizeof(float), cudaMemcpyDeviceToHost, h->stream),
+               "field download");
+        FC_RC(wait_stream(h, kTransferTimeoutMs));
+        std::memcpy(out + (cell0 + done) * 4, h->h_stage, nc * 4 * sizeof(float));
+    }
+    return FC_LBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fc_lbm_create(fc_lbm** out) {
+    if (!out) return FC_LBM_ERR_INVALID_ARG;
+    *out = new (std::nothrow) fc_lbm();
+    return *out ? FC_LBM_OK : FC_LBM_ERR_OUT_OF_MEMORY;
+}
+
+void fc_lbm_destroy(fc_lbm* h) {
+    if (!h) return;
+    if (h->valid || h->stream) {
+        DeviceGuard dg(h->device);
+        release(h);
+    }
+    delete h;
+}
+
+const char* fc_lbm_last_error(const fc_lbm* h) { return h ? h->err.c_str() : "null handle"; }
+
+int fc_lbm_shutdown(fc_lbm* h) {
+    if (!h) return FC_LBM_ERR_INVALID_ARG;
+    DeviceGuard dg(h->device);
+    release(h);
+    return FC_LBM_OK;
+}
+
+int fc_lbm_init(fc_lbm* h, const fc_grid_desc* grid, int32_t model, const fc_options* opts) {
+    if (!h) return FC_LBM_ERR_INVALID_ARG;
+    {
+        DeviceGuard dg(h->device);
+        release(h);  // LbmSolver::Init starts with Shutdown (LbmSolver.cpp:206)
+    }
+    h->err.clear();
+    if (!grid || !grid->solid) return fail(h, FC_LBM_ERR_INVALID_ARG, "grid and grid->solid are required");
+    if (grid->nx <= 0 || grid->ny <= 0 || grid->nz <= 0)
+        return fail(h, FC_LBM_ERR_INVALID_ARG, "grid dimensions must be positive");
+    if (model != FC_LATTICE_D3Q15 && model != FC_LATTICE_D3Q19)
+        return fail(h, FC_LBM_ERR_INVALID_ARG, "unknown lattice model");
+    fc_options o{0, FC_STORAGE_FP32, FC_STREAMING_PINGPONG, 0};
+    if (opts) o = *opts;
+    if (o.storage < FC_STORAGE_FP32 || o.storage > FC_STORAGE_BF16_OFFSET)
+        return fail(h, FC_LBM_ERR_INVALID_ARG, "unknown storage format");
+    if (o.streaming != FC_STREAMING_PINGPONG)
+        return fail(h, FC_LBM_ERR_UNSUPPORTED, "only ping-pong streaming is available in this build");
+    const size_t n = (size_t)grid->nx * (size_t)grid->ny * (size_t)grid->nz;
+    if (n >= (size_t(1) << 32))
+        return fail(h, FC_LBM_ERR_INVALID_ARG, "grid too large: at most 2^32-1 cells per lattice");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(h, FC_LBM_ERR_CUDA, "no CUDA device available");
+    if (o.device < 0 || o.device >= ndev) return fail(h, FC_LBM_ERR_INVALID_ARG, "device ordinal out of range");
+
+    h->device = o.device;
+    DeviceGuard dg(h->device);
+    h->model = model;
+    h->q = model == FC_LATTICE_D3Q19 ? 19 : 15;
+    h->storage = o.storage;
+    h->streaming = o.streaming;
+    h->g.nx = grid->nx;
+    h->g.ny = grid->ny;
+    h->g.nz = grid->nz;
+    h->g.wpr = (grid->nx + 31) / 32;
+    h->g.nxy = (long long)grid->nx * grid->ny;
+    h->g.n = n;
+
+    const size_t elem = h->storage == FC_STORAGE_FP32 ? 4 : 2;
+    const size_t pop_bytes = (size_t)h->q * n * elem;
+    const size_t bits_bytes = (size_t)grid->ny * grid->nz * h->g.wpr * sizeof(uint32_t);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+        const size_t need = 2 * pop_bytes + n * (1 + (grid->signed_distance ? 4 : 0)) + bits_bytes + n /*flags*/;
+        if (need > free_b) {
+            char buf[256];
+            std::snprintf(buf, sizeof(buf), "grid too large: %zu cells need %.2f GiB of device memory, %.2f GiB free",
+                          n, need / 1073741824.0, free_b / 1073741824.0);
+            return fail(h, FC_LBM_ERR_OUT_OF_MEMORY, buf);
+        }
+    }
+
+    auto init_body = [&]() -> int {
+        FC_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "create stream");
+        FC_TRY(h, cudaEventCreateWithFlags(&h->ev_own, cudaEventDisableTiming), "create event");
+        FC_TRY(h, cudaEventCreateWithFlags(&h->ev_foreign, cudaEventDisableTiming), "create event");
+        FC_TRY(h, cudaEventCreateWithFlags(&h->ev_sync, cudaEventDisableTiming), "create event");
+        h->stage_floats = kStageFloats;
+        FC_TRY(h, cudaMalloc(&h->d_stage, h->stage_floats * sizeof(float)), "alloc staging");
+        FC_TRY(h, cudaMallocHost(&h->h_stage, h->stage_floats * sizeof(float)), "alloc pinned staging");
+        FC_TRY(h, cudaMalloc(&h->pop[0], pop_bytes), "alloc populations");
+        FC_TRY(h, cudaMalloc(&h->pop[1], pop_bytes), "alloc populations");
+        FC_TRY(h, cudaMalloc(&h->d_solid, n), "alloc solid mask");
+        if (grid->signed_distance) FC_TRY(h, cudaMalloc(&h->d_sdf, n * sizeof(float)), "alloc SDF");
+        FC_TRY(h, cudaMalloc(&h->d_bulk_bits, bits_bytes), "alloc bulk mask");
+        FC_TRY(h, cudaMalloc(&h->d_diverged, sizeof(int)), "alloc divergence flag");
+        h->stats_blocks = fc::stats_blocks(h->g);
+        FC_TRY(h, cudaMalloc(&h->d_stats_partials, (size_t)h->stats_blocks * fc::kStatsSlots * sizeof(double)),
+               "alloc stats partials");
+        FC_TRY(h, cudaMalloc(&h->d_stats_result, fc::kStatsSlots * sizeof(double)), "alloc stats result");
+        FC_TRY(h, cudaMemsetAsync(h->d_diverged, 0, sizeof(int), h->stream), "clear flag");
+        const bool dev = grid->memory == FC_MEMORY_DEVICE;
+        FC_RC(upload(h, h->d_solid, grid->solid, n, dev));
+        if (grid->signed_distance) FC_RC(upload(h, h->d_sdf, grid->signed_distance, n * sizeof(float), dev));
+        FC_RC(build_boundary(h));
+        h->solid_cpu.resize(n);
+        if (dev) {
+            FC_TRY(h, cudaMemcpy(h->solid_cpu.data(), grid->solid, n, cudaMemcpyDeviceToHost), "copy solid mask");
+        } else {
+            std::memcpy(h->solid_cpu.data(), grid->solid, n);
+        }
+        // A defined state before the first Reset: quiescent equilibrium.
+        FC_TRY(h, fc::launch_seed_uniform(h->q, h->storage, h->pop[0], h->g, 1.0f, 0.0f, 0.0f, 0.0f, h->stream),
+               "seed");
+        h->launches++;
+        return wait_stream(h, kTransferTimeoutMs);
+    };
+    int rc = init_body();
+    if (rc != FC_LBM_OK) {
+        std::string keep = h->err;
+        release(h);
+        h->err = keep;
+        return rc;
+    }
+    h->cur = 0;
+    h->steps_since_reset = 0;
+    h->valid = true;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_reset(fc_lbm* h, const fc_params* params, int32_t seed_mid) {
+    FC_RC(check_ready(h));
+    if (!params_ok(params)) return fail(h, FC_LBM_ERR_INVALID_ARG, "invalid params (tau must exceed 0.5, Cs >= 0)");
+    DeviceGuard dg(h->device);
+    h->params = *params;
+    // LbmReference::Reset / LbmSolver::Reset seed (LbmReference.cpp:193-202).
+    float rho = 1.0f, ux = 0.0f;
+    if (seed_mid) {
+        const float u = h->params.inlet_velocity;
+        const float mid = 0.5f * u;
+        ux = h->params.reverse_flow ? -mid : mid;
+        const float dev = 0.5f * (u * u - mid * mid);
+        rho = 1.0f + 3.0f * dev;
+    }
+    FC_TRY(h, fc::launch_seed_uniform(h->q, h->storage, h->pop[0], h->g, rho, ux, 0.0f, 0.0f, h->stream), "seed");
+    FC_TRY(h, cudaMemsetAsync(h->d_diverged, 0, sizeof(int), h->stream), "clear flag");
+    h->launches++;
+    h->cur = 0;
+    h->steps_since_reset = 0;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_reset_from_field(fc_lbm* h, const float* field, size_t count) {
+    FC_RC(check_ready(h));
+    if (!field || count != h->g.n * 4)
+        return fail(h, FC_LBM_ERR_INVALID_ARG, "field must hold exactly 4 floats per cell");
+    DeviceGuard dg(h->device);
+    const size_t chunk = h->stage_floats / 4;
+    for (size_t c0 = 0; c0 < h->g.n; c0 += chunk) {
+        const size_t nc = std::min(chunk, h->g.n - c0);
+        FC_RC(wait_stream(h, kTransferTimeoutMs));
+        std::memcpy(h->h_stage, field + c0 * 4, nc * 4 * sizeof(float));
+        FC_TRY(h, cudaMemcpyAsync(h->d_stage, h->h_stage, nc * 4 * sizeof(float), cudaMemcpyHostToDevice, h->stream),
+               "field upload");
+        FC_TRY(h, fc::launch_seed_field(h->q, h->storage, h->pop[0], h->g, h->d_stage, h->d_solid, c0, nc, h->stream),
+               "seed from field");
+        h->launches++;
+    }
+    FC_TRY(h, cudaMemsetAsync(h->d_diverged, 0, sizeof(int), h->stream), "clear flag");
+    h->cur = 0;
+    h->steps_since_reset = 0;
+    return wait_stream(h, kTransferTimeoutMs);
+}
+
+int fc_lbm_set_params(fc_lbm* h, const fc_params* params) {
+    if (!h) return FC_LBM_ERR_INVALID_ARG;
+    if (!params_ok(params)) return fail(h, FC_LBM_ERR_INVALID_ARG, "invalid params (tau must exceed 0.5, Cs >= 0)");
+    h->params = *params;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_get_params(const fc_lbm* h, fc_params* out) {
+    if (!h || !out) return FC_LBM_ERR_INVALID_ARG;
+    *out = h->params;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_step(fc_lbm* h, void* stream, int32_t n) {
+    FC_RC(check_ready(h));
+    if (n < 0) return fail(h, FC_LBM_ERR_INVALID_ARG, "negative step count");
+    DeviceGuard dg(h->device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+    FC_RC(enter_stream(h, s));
+    for (int k = 0; k < n; ++k) {
+        FC_RC(step_range_on(h, s, 0, h->g.nz));
+        h->cur = 1 - h->cur;
+        h->steps_since_reset++;
+    }
+    return leave_stream(h, s);
+}
+
+int fc_lbm_step_range(fc_lbm* h, void* stream, int32_t z_start, int32_t z_count) {
+    FC_RC(check_ready(h));
+    DeviceGuard dg(h->device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+    FC_RC(enter_stream(h, s));
+    FC_RC(step_range_on(h, s, z_start, z_count));
+    return leave_stream(h, s);
+}
+
+int fc_lbm_advance_substep(fc_lbm* h) {
+    FC_RC(check_ready(h));
+    h->cur = 1 - h->cur;
+    h->steps_since_reset++;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_readback_field(fc_lbm* h, float* out, size_t count) {
+    FC_RC(check_ready(h));
+    if (!out || count != h->g.n * 4) return fail(h, FC_LBM_ERR_INVALID_ARG, "output must hold 4 floats per cell");
+    DeviceGuard dg(h->device);
+    return field_to_host(h, 0, h->g.n, out);
+}
+
+int fc_lbm_readback_field_range(fc_lbm* h, int32_t z_start, int32_t z_count, float* out, size_t count) {
+    FC_RC(check_ready(h));
+    if (!out || count != h->g.n * 4) return fail(h, FC_LBM_ERR_INVALID_ARG, "output must hold 4 floats per cell");
+    const int z1 = std::min(h->g.nz, z_start + z_count);
+    const int z0 = std::max(0, z_start);
+    if (z1 <= z0) return FC_LBM_OK;
+    DeviceGuard dg(h->device);
+    return field_to_host(h, (size_t)z0 * h->g.nxy, (size_t)(z1 - z0) * h->g.nxy, out);
+}
+
+int fc_lbm_readback_stats(fc_lbm* h, fc_stats* out) {
+    FC_RC(check_ready(h));
+    if (!out) return FC_LBM_ERR_INVALID_ARG;
+    DeviceGuard dg(h->device);
+    FC_TRY(h, fc::launch_stats(h->q, h->storage, h->pop[h->cur], h->d_solid, h->d_sdf, h->g, h->d_stats_partials,
+                               h->stats_blocks, h->d_stats_result, h->stream),
+           "stats kernel");
+    h->launches += 2;
+    FC_TRY(h, cudaMemcpyAsync(h->h_stage, h->d_stats_result, fc::kStatsSlots * sizeof(double), cudaMemcpyDeviceToHost,
+                              h->stream),
+           "stats download");
+    FC_RC(wait_stream(h, kTransferTimeoutMs));
+    double r[fc::kStatsSlots];
+    std::memcpy(r, h->h_stage, sizeof(r));
+    std::memset(out, 0, sizeof(*out));
+    const double fluid = r[6];
+    out->fluid_cells = (uint64_t)fluid;
+    out->density_sum = r[0];
+    out->speed_sum = r[1];
+    out->total_mass = r[2];
+    out->force_sum[0] = r[3];
+    out->force_sum[1] = r[4];
+    out->force_sum[2] = r[5];
+    if (fluid > 0) {
+        out->avg_density = (float)(r[0] / fluid);
+        out->avg_speed = (float)(r[1] / fluid);
+        out->min_density = (float)r[7];
+        out->max_density = (float)r[8];
+    }
+    out->max_speed = (float)r[9];
+    out->max_stress = (float)r[10];
+    out->force_x = (float)r[3];
+    out->force_y = (float)r[4];
+    out->force_z = (float)r[5];
+    out->has_nan = r[11] != 0.0;
+    out->valid = 1;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_probe_slice_health(fc_lbm* h, int32_t z, int32_t* diverged) {
+    FC_RC(check_ready(h));
+    if (!diverged) return FC_LBM_ERR_INVALID_ARG;
+    DeviceGuard dg(h->device);
+    const int gz = std::min(std::max(z, 0), h->g.nz - 1);  // LbmSolver.cpp:655
+    const size_t layer = (size_t)h->g.nxy;
+    const size_t c0 = (size_t)gz * layer;
+    *diverged = 0;
+    const size_t chunk = h->stage_floats / 4;
+    for (size_t done = 0; done < layer; done += chunk) {
+        const size_t nc = std::min(chunk, layer - done);
+        FC_TRY(h, fc::launch_field(h->q, h->storage, h->pop[h->cur], h->d_solid, h->d_sdf, h->g, c0 + done, nc,
+                                   h->d_stage, h->stream),
+               "field kernel");
+        h->launches++;
+        FC_TRY(h, cudaMemcpyAsync(h->h_stage, h->d_stage, nc * 4 * sizeof(float), cudaMemcpyDeviceToHost, h->stream),
+               "layer download");
+        FC_RC(wait_stream(h, kTransferTimeoutMs));
+        for (size_t i = 0; i < nc; ++i) {  // LbmSolver.cpp:699-716
+            const float* v = h->h_stage + i * 4;
+            if (!std::isfinite(v[0]) || !std::isfinite(v[1]) || !std::isfinite(v[2]) || !std::isfinite(v[3])) {
+                *diverged = 1;
+                return FC_LBM_OK;
+            }
+            if (!h->solid_cpu[c0 + done + i]) {
+                const float sp2 = v[1] * v[1] + v[2] * v[2] + v[3] * v[3];
+                if (v[0] <= 0.0f || sp2 > 4.0f) {
+                    *diverged = 1;
+                    return FC_LBM_OK;
+                }
+            }
+        }
+    }
+    return FC_LBM_OK;
+}
+
+int fc_lbm_has_diverged(fc_lbm* h, int32_t* diverged) {
+    FC_RC(check_ready(h));
+    if (!diverged) return FC_LBM_ERR_INVALID_ARG;
+    DeviceGuard dg(h->device);
+    FC_TRY(h, cudaMemcpyAsync(h->h_stage, h->d_diverged, sizeof(int), cudaMemcpyDeviceToHost, h->stream),
+           "flag download");
+    FC_RC(wait_stream(h, kTransferTimeoutMs));
+    int v = 0;
+    std::memcpy(&v, h->h_stage, sizeof(int));
+    *diverged = v != 0;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_copy_solid_mask(const fc_lbm* h, uint8_t* out, size_t count) {
+    if (!h || !out) return FC_LBM_ERR_INVALID_ARG;
+    if (!h->valid) return FC_LBM_ERR_NOT_INITIALIZED;
+    if (count != h->solid_cpu.size()) return FC_LBM_ERR_INVALID_ARG;
+    std::memcpy(out, h->solid_cpu.data(), count);
+    return FC_LBM_OK;
+}
+
+int fc_lbm_is_valid(const fc_lbm* h) { return h && h->valid ? 1 : 0; }
+
+int fc_lbm_model(const fc_lbm* h) { return h ? h->model : FC_LBM_ERR_INVALID_ARG; }
+
+int fc_lbm_dims(const fc_lbm* h, int32_t* nx, int32_t* ny, int32_t* nz) {
+    if (!h) return FC_LBM_ERR_INVALID_ARG;
+    if (nx) *nx = h->valid ? h->g.nx : 0;
+    if (ny) *ny = h->valid ? h->g.ny : 0;
+    if (nz) *nz = h->valid ? h->g.nz : 0;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_sync(fc_lbm* h, int32_t timeout_ms) {
+    FC_RC(check_ready(h));
+    DeviceGuard dg(h->device);
+    return wait_stream(h, timeout_ms);
+}
+
+int fc_lbm_get_stream(const fc_lbm* h, void** stream) {
+    if (!h || !stream) return FC_LBM_ERR_INVALID_ARG;
+    if (!h->valid) return FC_LBM_ERR_NOT_INITIALIZED;
+    *stream = (void*)h->stream;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_boundary_info(const fc_lbm* h, uint64_t* boundary_cells, uint64_t* bouzidi_links, uint64_t* bulk_cells) {
+    if (!h) return FC_LBM_ERR_INVALID_ARG;
+    if (boundary_cells) *boundary_cells = h->n_bnd;
+    if (bouzidi_links) *bouzidi_links = h->n_bz;
+    if (bulk_cells) *bulk_cells = h->n_bulk;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_step_timed(fc_lbm* h, int32_t n, float* total_ms, float* bulk_ms, float* boundary_ms) {
+    FC_RC(check_ready(h));
+    if (n < 0) return fail(h, FC_LBM_ERR_INVALID_ARG, "negative step count");
+    DeviceGuard dg(h->device);
+    std::vector<cudaEvent_t> ev((size_t)n * 4 + 2, nullptr);
+    auto destroy = [&]() {
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+    };
+    for (cudaEvent_t& e : ev) {
+        cudaError_t ce = cudaEventCreate(&e);
+        if (ce != cudaSuccess) {
+            destroy();
+            return cuda_fail(h, ce, "create timing event");
+        }
+    }
+    const uint32_t b = h->z_begin[0], e = h->z_begin[(size_t)h->g.nz];
+    fc::BoundaryList bl{h->d_cells, h->d_links, h->d_coef_off, h->d_coef};
+    int rc = FC_LBM_OK;
+    cudaEventRecord(ev[0], h->stream);
+    for (int k = 0; k < n && rc == FC_LBM_OK; ++k) {
+        const fc::StepParams p = step_params(h);
+        const void* fin = h->pop[h->cur];
+        void* fout = h->pop[1 - h->cur];
+        cudaEventRecord(ev[2 + 4 * k], h->stream);
+        cudaError_t ce = cudaSuccess;
+        if (h->n_bulk > 0) {
+            ce = fc::launch_bulk_pull(h->q, h->storage, fin, fout, h->d_bulk_bits, h->g, p, 0, h->g.nz, h->d_diverged,
+                                      h->stream);
+            h->launches++;
+        }
+        cudaEventRecord(ev[3 + 4 * k], h->stream);
+        cudaEventRecord(ev[4 + 4 * k], h->stream);
+        if (ce == cudaSuccess && e > b) {
+            ce = fc::launch_boundary_pull(h->q, h->storage, fin, fout, bl, b, e, h->g, p, h->d_diverged, h->stream);
+            h->launches++;
+        }
+        cudaEventRecord(ev[5 + 4 * k], h->stream);
+        if (ce != cudaSuccess) rc = cuda_fail(h, ce, "timed step");
+        h->cur = 1 - h->cur;
+        h->steps_since_reset++;
+    }
+    cudaEventRecord(ev[1], h->stream);
+    if (rc == FC_LBM_OK) rc = wait_stream(h, kTransferTimeoutMs);
+    if (rc == FC_LBM_OK) {
+        float t = 0.0f, tb = 0.0f, td = 0.0f, x = 0.0f;
+        cudaEventElapsedTime(&t, ev[0], ev[1]);
+        for (int k = 0; k < n; ++k) {
+            cudaEventElapsedTime(&x, ev[2 + 4 * k], ev[3 + 4 * k]);
+            tb += x;
+            cudaEventElapsedTime(&x, ev[4 + 4 * k], ev[5 + 4 * k]);
+            td += x;
+        }
+        if (total_ms) *total_ms = t;
+        if (bulk_ms) *bulk_ms = tb;
+        if (boundary_ms) *boundary_ms = td;
+    }
+    destroy();
+    return rc;
+}
+
+int fc_lbm_launch_count(const fc_lbm* h, uint64_t* launches) {
+    if (!h || !launches) return FC_LBM_ERR_INVALID_ARG;
+    *launches = h->launches;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_save_populations(fc_lbm* h, float* out, size_t count) {
+    FC_RC(check_ready(h));
+    if (!out || count != (size_t)h->q * h->g.n)
+        return fail(h, FC_LBM_ERR_INVALID_ARG, "output must hold Q floats per cell");
+    DeviceGuard dg(h->device);
+    const size_t chunk = h->stage_floats / (size_t)h->q;
+    const int solid_w = h->steps_since_reset > 0 ? 1 : 0;
+    for (size_t c0 = 0; c0 < h->g.n; c0 += chunk) {
+        const size_t nc = std::min(chunk, h->g.n - c0);
+        FC_TRY(h, fc::launch_pops_out(h->q, h->storage, h->pop[h->cur], h->d_solid, solid_w, h->g, c0, nc, h->d_stage,
+                                      h->stream),
+               "population readout");
+        h->launches++;
+        FC_TRY(h, cudaMemcpyAsync(h->h_stage, h->d_stage, nc * h->q * sizeof(float), cudaMemcpyDeviceToHost, h->stream),
+               "population download");
+        FC_RC(wait_stream(h, kTransferTimeoutMs));
+        for (int i = 0; i < h->q; ++i)
+            std::memcpy(out + (size_t)i * h->g.n + c0, h->h_stage + (size_t)i * nc, nc * sizeof(float));
+    }
+    return FC_LBM_OK;
+}
+
+int fc_lbm_load_populations(fc_lbm* h, const float* in, size_t count) {
+    FC_RC(check_ready(h));
+    if (!in || count != (size_t)h->q * h->g.n)
+        return fail(h, FC_LBM_ERR_INVALID_ARG, "input must hold Q floats per cell");
+    DeviceGuard dg(h->device);
+    const size_t chunk = h->stage_floats / (size_t)h->q;
+    for (size_t c0 = 0; c0 < h->g.n; c0 += chunk) {
+        const size_t nc = std::min(chunk, h->g.n - c0);
+        FC_RC(wait_stream(h, kTransferTimeoutMs));
+        for (int i = 0; i < h->q; ++i)
+            std::memcpy(h->h_stage + (size_t)i * nc, in + (size_t)i * h->g.n + c0, nc * sizeof(float));
+        FC_TRY(h, cudaMemcpyAsync(h->d_stage, h->h_stage, nc * h->q * sizeof(float), cudaMemcpyHostToDevice, h->stream),
+               "population upload");
+        FC_TRY(h, fc::launch_pops_in(h->q, h->storage, h->pop[h->cur], h->g, c0, nc, h->d_stage, h->stream),
+               "population write");
+        h->launches++;
+    }
+    // The loaded state is a post-step state: solid cells hold what was given.
+    h->steps_since_reset = 0;
+    return wait_stream(h, kTransferTimeoutMs);
+}
+
+}  // extern "C"

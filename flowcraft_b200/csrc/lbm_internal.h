@@ -1,0 +1,96 @@
+// Shared between the kernel translation units and the C-ABI host code.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace fc {
+
+// Grid geometry passed by value to every kernel.
+struct Geom {
+    int nx, ny, nz;
+    int wpr;        // 32-bit words per x-row of the bulk bitmask = ceil(nx/32)
+    long long nxy;  // nx*ny
+    size_t n;       // nx*ny*nz (SoA plane stride)
+};
+
+// Live parameters of one step (LbmSolver::Params, LbmSolver.h:61-100).
+struct StepParams {
+    float tau;
+    float cs;
+    float inlet_ux;  // signed: -inletVelocity when reverse_flow
+    int inlet_x;     // 0, or nx-1 when reverse_flow
+    int outlet_x;    // nx-1, or 0 when reverse_flow
+    int reverse;
+    int slip_y, slip_z;
+};
+
+// Per-link handling codes of a boundary-list cell, 3 bits per direction.
+enum LinkKind : unsigned {
+    kLinkStream = 0,   // upstream neighbour is interior fluid: plain pull
+    kLinkBounce = 1,   // plain halfway bounce-back: f_opp(x)
+    kLinkBzNear = 2,   // Bouzidi, q < 1/2: c1*f_opp(x) + c2*f_opp(x+e_i)
+    kLinkBzFar = 3,    // Bouzidi, q >= 1/2: c1*f_opp(x) + c2*f_i(x)
+    kLinkEdge = 4,     // off the Y/Z domain edge: free-slip mirror or bounce-back, decided per step
+};
+// Cell class, stored in bits 60..62 of the 64-bit link word.
+enum CellClass : unsigned {
+    kCellFluid = 0,      // fluid cell with at least one non-stream link
+    kCellPlane = 1,      // fluid cell on x = 0 or x = nx-1 (inlet or outlet this step)
+    kCellSolidFill = 2,  // solid cell at x = 1 or x = nx-2 (an outlet's neighbour)
+};
+constexpr int kClassShift = 60;
+
+// Device-side boundary list (sorted by cell index).
+struct BoundaryList {
+    const uint32_t* cells;
+    const unsigned long long* links;
+    const uint32_t* coef_off;
+    const float2* coef;
+};
+
+// ---- launchers (defined in the .cu files) ----
+// storage: 0 fp32, 1 fp16 offset, 2 bf16 offset; q: 15 or 19.
+cudaError_t launch_bulk_pull(int q, int storage, const void* fin, void* fout, const uint32_t* bulk_bits,
+                             const Geom& g, const StepParams& p, int z0, int zc, int* diverged, cudaStream_t s);
+cudaError_t launch_boundary_pull(int q, int storage, const void* fin, void* fout, const BoundaryList& bl,
+                                 uint32_t begin, uint32_t end, const Geom& g, const StepParams& p, int* diverged,
+                                 cudaStream_t s);
+
+cudaError_t launch_seed_uniform(int q, int storage, void* f, const Geom& g, float rho, float ux, float uy, float uz,
+                                cudaStream_t s);
+cudaError_t launch_seed_field(int q, int storage, void* f, const Geom& g, const float* field, const uint8_t* solid,
+                              size_t cell0, size_t cells, cudaStream_t s);
+
+cudaError_t launch_field(int q, int storage, const void* f, const uint8_t* solid, const float* sdf, const Geom& g,
+                         size_t cell0, size_t cells, float* out, cudaStream_t s);
+cudaError_t launch_pops_out(int q, int storage, const void* f, const uint8_t* solid, int solid_is_weight,
+                            const Geom& g, size_t cell0, size_t cells, float* out, cudaStream_t s);
+cudaError_t launch_pops_in(int q, int storage, void* f, const Geom& g, size_t cell0, size_t cells,
+                           const float* in, cudaStream_t s);
+
+// Stats: `partials` holds stats_partial_doubles() doubles per block of
+// stats_blocks(); `result` receives kStatsSlots doubles.
+constexpr int kStatsSlots = 12;
+int stats_blocks(const Geom& g);
+cudaError_t launch_stats(int q, int storage, const void* f, const uint8_t* solid, const float* sdf, const Geom& g,
+                         double* partials, int blocks, double* result, cudaStream_t s);
+
+// Setup (geometry classification and boundary-list construction).
+// counts[0] += flagged (boundary-list) cells, counts[1] += bulk cells.
+cudaError_t launch_classify(int q, const uint8_t* solid, const Geom& g, uint8_t* flags, uint32_t* bulk_bits,
+                            unsigned long long* counts, cudaStream_t s);
+cudaError_t launch_links(int q, const uint32_t* cells, size_t count, const uint8_t* solid, const float* sdf,
+                         const Geom& g, unsigned long long* links, uint32_t* nbz, const uint32_t* coef_off,
+                         float2* coef, cudaStream_t s);
+cudaError_t launch_z_offsets(const uint32_t* cells, size_t count, const Geom& g, uint32_t* z_begin, cudaStream_t s);
+// Ordered stream compaction of flagged cell indices (CUB); temp sized by the
+// first call with temp == nullptr.
+cudaError_t select_flagged_cells(void* temp, size_t& temp_bytes, const uint8_t* flags, uint32_t* out,
+                                 uint32_t* count_out, size_t n, cudaStream_t s);
+cudaError_t exclusive_scan_u32(void* temp, size_t& temp_bytes, const uint32_t* in, uint32_t* out, size_t n,
+                               cudaStream_t s);
+
+}  // namespace fc

@@ -1,0 +1,325 @@
+// Readback kernels: macroscopic field, raw populations, and the FP64
+// statistics reduction.
+//
+// The field follows LbmReference::ReadbackField (LbmReference.cpp:475-500):
+// fluid cells get (rho, ux, uy, uz) from the current post-collision state;
+// solid cells get the momentum-exchange force of their fluid neighbours,
+// (|F| / (6 sum w), Fx, Fy, Fz) (LbmReference::SolidCellForce,
+// LbmReference.cpp:127-148), with the same Bouzidi reconstruction the step
+// uses. Only the moments are computed — the step never writes a
+// 16-byte-per-cell macro buffer the way the reference's GPU kernel does
+// (shaders/lbm_step.comp.glsl:360-363), which saves 16 B of HBM traffic per
+// cell update.
+#include "collide.cuh"
+#include "lbm_internal.h"
+#include "storage.cuh"
+
+namespace fc {
+
+__device__ __forceinline__ bool inb(const Geom& g, int x, int y, int z) {
+    return x >= 0 && y >= 0 && z >= 0 && x < g.nx && y < g.ny && z < g.nz;
+}
+__device__ __forceinline__ size_t cidx(const Geom& g, int x, int y, int z) { return ((size_t)z * g.ny + y) * g.nx + x; }
+
+// InterpolatedBounceBack for fluid node a (cell ca) whose direction-i
+// upstream neighbour s (cell cs) is solid (LbmReference.cpp:100-122).
+template <int Q, class S, int I>
+__device__ float bounce_rt(const typename S::T* __restrict__ f, const uint8_t* __restrict__ solid,
+                           const float* __restrict__ sdf, const Geom& g, int ax, int ay, int az, size_t ca,
+                           size_t cs) {
+    using L = Lattice<Q>;
+    constexpr int op = L::opp(I);
+    const float plain = load_pop_c<Q, S, op>(f, g.n, ca);
+    if (!sdf) return plain;
+    const float phi_f = sdf[ca], phi_s = sdf[cs];
+    if (!isfinite(phi_f) || !isfinite(phi_s)) return plain;
+    const float denom = phi_f - phi_s;
+    if (!(denom > 1e-4f)) return plain;
+    float q = phi_f / denom;
+    q = (q < 0.0f) ? 0.0f : ((1.0f < q) ? 1.0f : q);
+    if (q < 0.5f) {
+        const int fx = ax + L::ex(I), fy = ay + L::ey(I), fz = az + L::ez(I);
+        if (!inb(g, fx, fy, fz) || solid[cidx(g, fx, fy, fz)]) return plain;
+        return 2.0f * q * plain + (1.0f - 2.0f * q) * load_pop_c<Q, S, op>(f, g.n, cidx(g, fx, fy, fz));
+    }
+    const float inv = 1.0f / (2.0f * q);
+    return inv * plain + (1.0f - inv) * load_pop_c<Q, S, I>(f, g.n, ca);
+}
+
+template <int Q, class S>
+__device__ float4 solid_force(const typename S::T* __restrict__ f, const uint8_t* __restrict__ solid,
+                              const float* __restrict__ sdf, const Geom& g, int x, int y, int z, size_t c) {
+    using L = Lattice<Q>;
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f, ws = 0.0f;
+    static_for<1, Q>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        constexpr int X = L::ex(i), Y = L::ey(i), Z = L::ez(i);
+        const int ax = x + X, ay = y + Y, az = z + Z;
+        if (!inb(g, ax, ay, az)) return;
+        const size_t ca = cidx(g, ax, ay, az);
+        if (solid[ca]) return;
+        const float plain = load_pop_c<Q, S, L::opp(i)>(f, g.n, ca);
+        const float bounced = bounce_rt<Q, S, i>(f, solid, sdf, g, ax, ay, az, ca, c);
+        const float dp = (plain + bounced) - 2.0f * L::w(i);
+        if constexpr (X > 0) fx = fx - dp;
+        if constexpr (X < 0) fx = fx + dp;
+        if constexpr (Y > 0) fy = fy - dp;
+        if constexpr (Y < 0) fy = fy + dp;
+        if constexpr (Z > 0) fz = fz - dp;
+        if constexpr (Z < 0) fz = fz + dp;
+        ws = ws + L::w(i);
+    });
+    const float mag = sqrtf((fx * fx + fy * fy) + fz * fz);
+    const float stress = (ws > 0.0f) ? (mag / (6.0f * ws)) : 0.0f;
+    return make_float4(stress, fx, fy, fz);
+}
+
+template <int Q, class S>
+__device__ __forceinline__ float4 fluid_moments(const typename S::T* __restrict__ f, const Geom& g, size_t c) {
+    float p[Q];
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        p[i] = load_pop_c<Q, S, i>(f, g.n, c);
+    });
+    float rho, ux, uy, uz;
+    moments<Q>(p, rho, ux, uy, uz);
+    return make_float4(rho, ux, uy, uz);
+}
+
+template <int Q, class S>
+__global__ void __launch_bounds__(256) k_field(const typename S::T* __restrict__ f, const uint8_t* __restrict__ solid,
+                                                const float* __restrict__ sdf, Geom g, size_t cell0, size_t cells,
+                                                float4* __restrict__ out) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= cells) return;
+    const size_t c = cell0 + k;
+    const int z = (int)(c / (size_t)g.nxy);
+    const size_t rem = c - (size_t)z * g.nxy;
+    const int y = (int)(rem / g.nx);
+    const int x = (int)(rem - (size_t)y * g.nx);
+    out[k] = solid[c] ? solid_force<Q, S>(f, solid, sdf, g, x, y, z, c) : fluid_moments<Q, S>(f, g, c);
+}
+
+template <int Q, class S>
+__global__ void k_pops_out(const typename S::T* __restrict__ f, const uint8_t* __restrict__ solid,
+                           int solid_is_weight, Geom g, size_t cell0, size_t cells, float* __restrict__ out) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= cells) return;
+    const size_t c = cell0 + k;
+    const bool sw = solid_is_weight && solid[c];
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        out[(size_t)i * cells + k] = sw ? Lattice<Q>::w(i) : load_pop_c<Q, S, i>(f, g.n, c);
+    });
+}
+
+template <int Q, class S>
+__global__ void k_pops_in(typename S::T* __restrict__ f, Geom g, size_t cell0, size_t cells,
+                          const float* __restrict__ in) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= cells) return;
+    const size_t c = cell0 + k;
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        store_pop_c<Q, S, i>(f, g.n, c, in[(size_t)i * cells + k]);
+    });
+}
+
+// ---- statistics (LbmReference::ComputeStats, LbmReference.cpp:502-585) ----
+// Slots: 0 density sum, 1 speed sum, 2 mass, 3..5 force sums, 6 fluid count,
+// 7 min density, 8 max density, 9 max speed, 10 max stress, 11 NaN flag.
+constexpr int kStatsThreads = 256;
+
+struct StatAcc {
+    double dsum = 0.0, ssum = 0.0, fx = 0.0, fy = 0.0, fz = 0.0, count = 0.0;
+    float mn = 1e30f, mx = -1e30f, vmax = 0.0f, smax = 0.0f;
+    int nan = 0;
+};
+
+__device__ __forceinline__ void stat_merge(StatAcc& a, const StatAcc& b) {
+    a.dsum += b.dsum;
+    a.ssum += b.ssum;
+    a.fx += b.fx;
+    a.fy += b.fy;
+    a.fz += b.fz;
+    a.count += b.count;
+    a.mn = fminf(a.mn, b.mn);
+    a.mx = fmaxf(a.mx, b.mx);
+    a.vmax = fmaxf(a.vmax, b.vmax);
+    a.smax = fmaxf(a.smax, b.smax);
+    a.nan |= b.nan;
+}
+
+__device__ __forceinline__ void stat_block_reduce(StatAcc& acc, double* out) {
+    __shared__ StatAcc sh[kStatsThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        StatAcc b;
+        b.dsum = __shfl_down_sync(0xffffffffu, acc.dsum, o);
+        b.ssum = __shfl_down_sync(0xffffffffu, acc.ssum, o);
+        b.fx = __shfl_down_sync(0xffffffffu, acc.fx, o);
+        b.fy = __shfl_down_sync(0xffffffffu, acc.fy, o);
+        b.fz = __shfl_down_sync(0xffffffffu, acc.fz, o);
+        b.count = __shfl_down_sync(0xffffffffu, acc.count, o);
+        b.mn = __shfl_down_sync(0xffffffffu, acc.mn, o);
+        b.mx = __shfl_down_sync(0xffffffffu, acc.mx, o);
+        b.vmax = __shfl_down_sync(0xffffffffu, acc.vmax, o);
+        b.smax = __shfl_down_sync(0xffffffffu, acc.smax, o);
+        b.nan = __shfl_down_sync(0xffffffffu, acc.nan, o);
+        stat_merge(acc, b);
+    }
+    if (lane == 0) sh[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        StatAcc t = sh[0];
+        for (int w = 1; w < kStatsThreads / 32; ++w) stat_merge(t, sh[w]);
+        out[0] = t.dsum;
+        out[1] = t.ssum;
+        out[2] = t.dsum;  // mass: the reference sums rho over fluid cells
+        out[3] = t.fx;
+        out[4] = t.fy;
+        out[5] = t.fz;
+        out[6] = t.count;
+        out[7] = t.mn;
+        out[8] = t.mx;
+        out[9] = t.vmax;
+        out[10] = t.smax;
+        out[11] = t.nan;
+    }
+}
+
+template <int Q, class S>
+__global__ void __launch_bounds__(kStatsThreads) k_stats(const typename S::T* __restrict__ f,
+                                                         const uint8_t* __restrict__ solid,
+                                                         const float* __restrict__ sdf, Geom g,
+                                                         double* __restrict__ partials) {
+    StatAcc acc;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < g.n; c += (size_t)gridDim.x * blockDim.x) {
+        if (solid[c]) {
+            const int z = (int)(c / (size_t)g.nxy);
+            const size_t rem = c - (size_t)z * g.nxy;
+            const int y = (int)(rem / g.nx);
+            const int x = (int)(rem - (size_t)y * g.nx);
+            const float4 v = solid_force<Q, S>(f, solid, sdf, g, x, y, z, c);
+            if (isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(v.w)) {
+                acc.fx += (double)v.y;
+                acc.fy += (double)v.z;
+                acc.fz += (double)v.w;
+                acc.smax = fmaxf(acc.smax, v.x);
+            }
+            continue;
+        }
+        const float4 m = fluid_moments<Q, S>(f, g, c);
+        if (!isfinite(m.x) || !isfinite(m.y) || !isfinite(m.z) || !isfinite(m.w)) {
+            acc.nan = 1;
+            continue;
+        }
+        const float sp = sqrtf(speed2(m.y, m.z, m.w));
+        acc.mn = fminf(acc.mn, m.x);
+        acc.mx = fmaxf(acc.mx, m.x);
+        acc.vmax = fmaxf(acc.vmax, sp);
+        acc.dsum += (double)m.x;
+        acc.ssum += (double)sp;
+        acc.count += 1.0;
+    }
+    stat_block_reduce(acc, partials + (size_t)blockIdx.x * kStatsSlots);
+}
+
+__global__ void __launch_bounds__(kStatsThreads) k_stats_final(const double* __restrict__ partials, int blocks,
+                                                               double* __restrict__ result) {
+    StatAcc acc;
+    for (int b = threadIdx.x; b < blocks; b += blockDim.x) {
+        const double* p = partials + (size_t)b * kStatsSlots;
+        StatAcc t;
+        t.dsum = p[0];
+        t.ssum = p[1];
+        t.fx = p[3];
+        t.fy = p[4];
+        t.fz = p[5];
+        t.count = p[6];
+        t.mn = (float)p[7];
+        t.mx = (float)p[8];
+        t.vmax = (float)p[9];
+        t.smax = (float)p[10];
+        t.nan = p[11] != 0.0;
+        stat_merge(acc, t);
+    }
+    stat_block_reduce(acc, result);
+}
+
+int stats_blocks(const Geom& g) {
+    const size_t want = (g.n + kStatsThreads * 8 - 1) / (kStatsThreads * 8);
+    const size_t cap = 148 * 16;
+    return (int)(want < 1 ? 1 : (want > cap ? cap : want));
+}
+
+template <int Q, class S>
+static cudaError_t field_t(const void* f, const uint8_t* solid, const float* sdf, const Geom& g, size_t cell0,
+                           size_t cells, float* out, cudaStream_t s) {
+    if (cells == 0) return cudaSuccess;
+    k_field<Q, S><<<(unsigned)((cells + 255) / 256), 256, 0, s>>>((const typename S::T*)f, solid, sdf, g, cell0, cells,
+                                                                  (float4*)out);
+    return cudaGetLastError();
+}
+
+template <int Q, class S>
+static cudaError_t pops_out_t(const void* f, const uint8_t* solid, int sw, const Geom& g, size_t cell0, size_t cells,
+                              float* out, cudaStream_t s) {
+    if (cells == 0) return cudaSuccess;
+    k_pops_out<Q, S><<<(unsigned)((cells + 255) / 256), 256, 0, s>>>((const typename S::T*)f, solid, sw, g, cell0,
+                                                                     cells, out);
+    return cudaGetLastError();
+}
+
+template <int Q, class S>
+static cudaError_t pops_in_t(void* f, const Geom& g, size_t cell0, size_t cells, const float* in, cudaStream_t s) {
+    if (cells == 0) return cudaSuccess;
+    k_pops_in<Q, S><<<(unsigned)((cells + 255) / 256), 256, 0, s>>>((typename S::T*)f, g, cell0, cells, in);
+    return cudaGetLastError();
+}
+
+template <int Q, class S>
+static cudaError_t stats_t(const void* f, const uint8_t* solid, const float* sdf, const Geom& g, double* partials,
+                           int blocks, double* result, cudaStream_t s) {
+    k_stats<Q, S><<<blocks, kStatsThreads, 0, s>>>((const typename S::T*)f, solid, sdf, g, partials);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_stats_final<<<1, kStatsThreads, 0, s>>>(partials, blocks, result);
+    return cudaGetLastError();
+}
+
+#define FC_DISPATCH(q, storage, FN, ...)                               \
+    do {                                                               \
+        if ((q) == 19) {                                               \
+            if ((storage) == 0) return FN<19, StoreF32>(__VA_ARGS__);  \
+            if ((storage) == 1) return FN<19, StoreF16>(__VA_ARGS__);  \
+            if ((storage) == 2) return FN<19, StoreBF16>(__VA_ARGS__); \
+        } else if ((q) == 15) {                                        \
+            if ((storage) == 0) return FN<15, StoreF32>(__VA_ARGS__);  \
+            if ((storage) == 1) return FN<15, StoreF16>(__VA_ARGS__);  \
+            if ((storage) == 2) return FN<15, StoreBF16>(__VA_ARGS__); \
+        }                                                              \
+        return cudaErrorInvalidValue;                                  \
+    } while (0)
+
+cudaError_t launch_field(int q, int storage, const void* f, const uint8_t* solid, const float* sdf, const Geom& g,
+                         size_t cell0, size_t cells, float* out, cudaStream_t s) {
+    FC_DISPATCH(q, storage, field_t, f, solid, sdf, g, cell0, cells, out, s);
+}
+
+cudaError_t launch_pops_out(int q, int storage, const void* f, const uint8_t* solid, int solid_is_weight,
+                            const Geom& g, size_t cell0, size_t cells, float* out, cudaStream_t s) {
+    FC_DISPATCH(q, storage, pops_out_t, f, solid, solid_is_weight, g, cell0, cells, out, s);
+}
+
+cudaError_t launch_pops_in(int q, int storage, void* f, const Geom& g, size_t cell0, size_t cells, const float* in,
+                           cudaStream_t s) {
+    FC_DISPATCH(q, storage, pops_in_t, f, g, cell0, cells, in, s);
+}
+
+cudaError_t launch_stats(int q, int storage, const void* f, const uint8_t* solid, const float* sdf, const Geom& g,
+                         double* partials, int blocks, double* result, cudaStream_t s) {
+    FC_DISPATCH(q, storage, stats_t, f, solid, sdf, g, partials, blocks, result, s);
+}
+
+}  // namespace fc

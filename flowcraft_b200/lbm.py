@@ -1,0 +1,422 @@
+"""Python host mirror of FlowCraft's ``LbmSolver`` (FlowCraft/LbmSolver.h:59-230)
+over the C ABI of ``libfc_lbm.so`` (include/fc_lbm.h).
+
+Method names, argument meanings and error behaviour follow the reference:
+``Init`` returns a bool and sets ``LastError()``; ``ResetFromField`` with a
+mis-sized field is ignored; ``Step``/``StepRange`` only enqueue; readbacks
+block. ``cmd`` arguments (an SDL_GPUCommandBuffer in the reference) are a
+CUDA stream here: ``None`` means the solver's own stream, or pass an int
+handle / ``torch.cuda.Stream``.
+
+There is no CPU fallback: importing works without a GPU, but every solver
+call goes to the CUDA library and fails loudly if it is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfc_lbm.so")
+
+FC_LBM_OK = 0
+FC_LBM_ERR_INVALID_ARG = -1
+FC_LBM_ERR_OUT_OF_MEMORY = -2
+FC_LBM_ERR_CUDA = -3
+FC_LBM_ERR_TIMEOUT = -4
+FC_LBM_ERR_NOT_INITIALIZED = -5
+FC_LBM_ERR_UNSUPPORTED = -6
+
+FC_MEMORY_HOST = 0
+FC_MEMORY_DEVICE = 1
+
+
+class LatticeModel(enum.IntEnum):
+    """FlowCraft/LatticeModel.h:12 — same enumerator order."""
+    D3Q15 = 0
+    D3Q19 = 1
+
+
+class Storage(enum.IntEnum):
+    FP32 = 0
+    FP16_OFFSET = 1
+    BF16_OFFSET = 2
+
+
+class Streaming(enum.IntEnum):
+    PINGPONG = 0
+    AA = 1
+
+
+class _GridDesc(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+        ("cell_size", ctypes.c_float), ("origin", ctypes.c_float * 3),
+        ("solid", ctypes.c_void_p), ("signed_distance", ctypes.c_void_p),
+        ("memory", ctypes.c_int32),
+    ]
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [
+        ("tau", ctypes.c_float), ("inlet_velocity", ctypes.c_float),
+        ("reverse_flow", ctypes.c_int32), ("free_slip_y", ctypes.c_int32),
+        ("free_slip_z", ctypes.c_int32), ("smagorinsky_cs", ctypes.c_float),
+    ]
+
+
+class _Options(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("storage", ctypes.c_int32),
+                ("streaming", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [
+        ("avg_density", ctypes.c_float), ("min_density", ctypes.c_float), ("max_density", ctypes.c_float),
+        ("avg_speed", ctypes.c_float), ("max_speed", ctypes.c_float),
+        ("force_x", ctypes.c_float), ("force_y", ctypes.c_float), ("force_z", ctypes.c_float),
+        ("max_stress", ctypes.c_float), ("has_nan", ctypes.c_int32), ("valid", ctypes.c_int32),
+        ("total_mass", ctypes.c_double), ("force_sum", ctypes.c_double * 3),
+        ("density_sum", ctypes.c_double), ("speed_sum", ctypes.c_double),
+        ("fluid_cells", ctypes.c_uint64),
+    ]
+
+
+# Every function the header declares, with its ctypes signature.
+_P = ctypes.c_void_p
+_I32 = ctypes.c_int32
+_SZ = ctypes.c_size_t
+_FP = ctypes.POINTER(ctypes.c_float)
+_U64P = ctypes.POINTER(ctypes.c_uint64)
+_I32P = ctypes.POINTER(ctypes.c_int32)
+SIGNATURES = {
+    "fc_lbm_create": (ctypes.c_int, [ctypes.POINTER(_P)]),
+    "fc_lbm_destroy": (None, [_P]),
+    "fc_lbm_init": (ctypes.c_int, [_P, ctypes.POINTER(_GridDesc), _I32, ctypes.POINTER(_Options)]),
+    "fc_lbm_shutdown": (ctypes.c_int, [_P]),
+    "fc_lbm_last_error": (ctypes.c_char_p, [_P]),
+    "fc_lbm_reset": (ctypes.c_int, [_P, ctypes.POINTER(_Params), _I32]),
+    "fc_lbm_reset_from_field": (ctypes.c_int, [_P, _FP, _SZ]),
+    "fc_lbm_set_params": (ctypes.c_int, [_P, ctypes.POINTER(_Params)]),
+    "fc_lbm_get_params": (ctypes.c_int, [_P, ctypes.POINTER(_Params)]),
+    "fc_lbm_step": (ctypes.c_int, [_P, _P, _I32]),
+    "fc_lbm_step_range": (ctypes.c_int, [_P, _P, _I32, _I32]),
+    "fc_lbm_advance_substep": (ctypes.c_int, [_P]),
+    "fc_lbm_readback_field": (ctypes.c_int, [_P, _FP, _SZ]),
+    "fc_lbm_readback_field_range": (ctypes.c_int, [_P, _I32, _I32, _FP, _SZ]),
+    "fc_lbm_readback_stats": (ctypes.c_int, [_P, ctypes.POINTER(_Stats)]),
+    "fc_lbm_probe_slice_health": (ctypes.c_int, [_P, _I32, _I32P]),
+    "fc_lbm_has_diverged": (ctypes.c_int, [_P, _I32P]),
+    "fc_lbm_copy_solid_mask": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint8), _SZ]),
+    "fc_lbm_is_valid": (ctypes.c_int, [_P]),
+    "fc_lbm_model": (ctypes.c_int, [_P]),
+    "fc_lbm_dims": (ctypes.c_int, [_P, _I32P, _I32P, _I32P]),
+    "fc_lbm_sync": (ctypes.c_int, [_P, _I32]),
+    "fc_lbm_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
+    "fc_lbm_boundary_info": (ctypes.c_int, [_P, _U64P, _U64P, _U64P]),
+    "fc_lbm_launch_count": (ctypes.c_int, [_P, _U64P]),
+    "fc_lbm_step_timed": (ctypes.c_int, [_P, _I32, _FP, _FP, _FP]),
+    "fc_lbm_save_populations": (ctypes.c_int, [_P, _FP, _SZ]),
+    "fc_lbm_load_populations": (ctypes.c_int, [_P, _FP, _SZ]),
+}
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads libfc_lbm.so and binds every entry point; raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"CUDA library not built: {path} (run python -m flowcraft_b200.build)")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class LbmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{msg} (status {code})")
+        self.code = code
+
+
+@dataclass
+class Params:
+    """LbmSolver::Params (LbmSolver.h:61-100), same defaults."""
+    tau: float = 0.8
+    inletVelocity: float = 0.05
+    reverseFlow: bool = False
+    freeSlipY: bool = True
+    freeSlipZ: bool = True
+    smagorinskyCs: float = 0.12
+
+    def _c(self) -> _Params:
+        return _Params(self.tau, self.inletVelocity, int(self.reverseFlow), int(self.freeSlipY),
+                       int(self.freeSlipZ), self.smagorinskyCs)
+
+
+@dataclass
+class VoxelGrid:
+    """FlowCraft/VoxelGrid.h:13-61. ``solid`` / ``signedDistance`` are flat
+    (or (nz, ny, nx)) numpy arrays, or CUDA torch tensors for device input."""
+    nx: int = 0
+    ny: int = 0
+    nz: int = 0
+    cellSize: float = 1.0
+    origin: tuple = (0.0, 0.0, 0.0)
+    solid: object = None
+    signedDistance: object = None
+
+    def CellCount(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    def Index(self, x: int, y: int, z: int) -> int:
+        return (z * self.ny + y) * self.nx + x
+
+
+@dataclass
+class Stats:
+    """LbmSolver::Stats (LbmSolver.h:172-184) plus the FP64 sums."""
+    avgDensity: float = 0.0
+    minDensity: float = 0.0
+    maxDensity: float = 0.0
+    avgSpeed: float = 0.0
+    maxSpeed: float = 0.0
+    forceX: float = 0.0
+    forceY: float = 0.0
+    forceZ: float = 0.0
+    maxStress: float = 0.0
+    hasNaN: bool = False
+    valid: bool = False
+    totalMass: float = 0.0
+    forceSum: tuple = (0.0, 0.0, 0.0)
+    fluidCells: int = 0
+    extra: dict = field(default_factory=dict)
+
+
+def _stream_ptr(cmd) -> int | None:
+    if cmd is None:
+        return None
+    if isinstance(cmd, int):
+        return cmd
+    handle = getattr(cmd, "cuda_stream", None)  # torch.cuda.Stream
+    if handle is not None:
+        return int(handle)
+    raise TypeError("cmd must be None, an int cudaStream_t or a torch.cuda.Stream")
+
+
+class LbmSolver:
+    """CUDA-backed drop-in for the reference's SDL_GPU ``LbmSolver``."""
+
+    def __init__(self):
+        self._lib = load_library()
+        h = ctypes.c_void_p()
+        rc = self._lib.fc_lbm_create(ctypes.byref(h))
+        if rc != FC_LBM_OK:
+            raise LbmError(rc, "fc_lbm_create failed")
+        self._h = h
+        self._solid_cpu = np.zeros(0, dtype=np.uint8)
+        self._model = LatticeModel.D3Q19
+        self._keep = []
+
+    # -- lifetime --------------------------------------------------------
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                self._lib.fc_lbm_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+    def close(self):
+        if self._h:
+            self._lib.fc_lbm_destroy(self._h)
+            self._h = None
+
+    def _check(self, rc: int, what: str):
+        if rc != FC_LBM_OK:
+            raise LbmError(rc, f"{what}: {self.LastError()}")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def Init(self, device, grid: VoxelGrid, model: LatticeModel = LatticeModel.D3Q19,
+             storage: Storage = Storage.FP32, streaming: Streaming = Streaming.PINGPONG) -> bool:
+        """LbmSolver::Init (LbmSolver.cpp:205-366); ``device`` is a CUDA ordinal."""
+        desc = _GridDesc()
+        desc.nx, desc.ny, desc.nz = grid.nx, grid.ny, grid.nz
+        desc.cell_size = grid.cellSize
+        desc.origin[:] = list(grid.origin)
+        solid, sdf = grid.solid, grid.signedDistance
+        keep = []
+        if hasattr(solid, "data_ptr"):  # torch tensor on a CUDA device
+            desc.memory = FC_MEMORY_DEVICE
+            solid = solid.contiguous()
+            desc.solid = solid.data_ptr()
+            keep.append(solid)
+            if sdf is not None and sdf.numel() == grid.CellCount():
+                sdf = sdf.contiguous()
+                desc.signed_distance = sdf.data_ptr()
+                keep.append(sdf)
+            self._solid_cpu = None
+        else:
+            desc.memory = FC_MEMORY_HOST
+            solid = np.ascontiguousarray(np.asarray(solid, dtype=np.uint8).ravel())
+            desc.solid = solid.ctypes.data
+            keep.append(solid)
+            # a mis-sized SDF is treated as absent (LbmReference.cpp:162-166)
+            if sdf is not None and np.asarray(sdf).size == grid.CellCount():
+                sdf = np.ascontiguousarray(np.asarray(sdf, dtype=np.float32).ravel())
+                desc.signed_distance = sdf.ctypes.data
+                keep.append(sdf)
+            self._solid_cpu = solid.copy()
+        opts = _Options(int(device), int(storage), int(streaming), 0)
+        rc = self._lib.fc_lbm_init(self._h, ctypes.byref(desc), int(model), ctypes.byref(opts))
+        if rc == FC_LBM_OK:
+            self._model = LatticeModel(model)
+            if self._solid_cpu is None:
+                self._solid_cpu = np.empty(grid.CellCount(), dtype=np.uint8)
+                self._check(self._lib.fc_lbm_copy_solid_mask(
+                    self._h, self._solid_cpu.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+                    self._solid_cpu.size), "copy solid mask")
+        return rc == FC_LBM_OK
+
+    def Shutdown(self):
+        self._lib.fc_lbm_shutdown(self._h)
+
+    def LastError(self) -> str:
+        return self._lib.fc_lbm_last_error(self._h).decode()
+
+    # -- state -----------------------------------------------------------
+    def Reset(self, params: Params, seedAtMidSpeed: bool = False):
+        self._check(self._lib.fc_lbm_reset(self._h, ctypes.byref(params._c()), int(seedAtMidSpeed)), "Reset")
+
+    def ResetFromField(self, field) -> None:
+        """Silently ignores a field of the wrong size, like LbmSolver.cpp:430."""
+        f = np.ascontiguousarray(np.asarray(field, dtype=np.float32).ravel())
+        rc = self._lib.fc_lbm_reset_from_field(self._h, f.ctypes.data_as(_FP), f.size)
+        if rc not in (FC_LBM_OK, FC_LBM_ERR_INVALID_ARG):
+            self._check(rc, "ResetFromField")
+
+    def SetParams(self, params: Params) -> None:
+        self._check(self._lib.fc_lbm_set_params(self._h, ctypes.byref(params._c())), "SetParams")
+
+    def GetParams(self) -> Params:
+        p = _Params()
+        self._check(self._lib.fc_lbm_get_params(self._h, ctypes.byref(p)), "GetParams")
+        return Params(p.tau, p.inlet_velocity, bool(p.reverse_flow), bool(p.free_slip_y), bool(p.free_slip_z),
+                      p.smagorinsky_cs)
+
+    # -- stepping --------------------------------------------------------
+    def Step(self, cmd, numSubsteps: int):
+        self._check(self._lib.fc_lbm_step(self._h, _stream_ptr(cmd), int(numSubsteps)), "Step")
+
+    def StepRange(self, cmd, zStart: int, zCount: int):
+        self._check(self._lib.fc_lbm_step_range(self._h, _stream_ptr(cmd), int(zStart), int(zCount)), "StepRange")
+
+    def AdvanceSubstep(self):
+        self._check(self._lib.fc_lbm_advance_substep(self._h), "AdvanceSubstep")
+
+    def Sync(self, timeout_ms: int = -1):
+        self._check(self._lib.fc_lbm_sync(self._h, int(timeout_ms)), "Sync")
+
+    # -- readback --------------------------------------------------------
+    def ReadbackField(self) -> np.ndarray:
+        out = np.empty(self.CellCount() * 4, dtype=np.float32)
+        self._check(self._lib.fc_lbm_readback_field(self._h, out.ctypes.data_as(_FP), out.size), "ReadbackField")
+        return out
+
+    def ReadbackFieldRange(self, zStart: int, zCount: int, outField: np.ndarray) -> None:
+        if outField.dtype != np.float32 or not outField.flags.c_contiguous:
+            raise TypeError("outField must be a contiguous float32 array of 4*CellCount()")
+        self._check(self._lib.fc_lbm_readback_field_range(self._h, int(zStart), int(zCount),
+                                                          outField.ctypes.data_as(_FP), outField.size),
+                    "ReadbackFieldRange")
+
+    def ReadbackStats(self) -> Stats:
+        s = _Stats()
+        self._check(self._lib.fc_lbm_readback_stats(self._h, ctypes.byref(s)), "ReadbackStats")
+        return Stats(s.avg_density, s.min_density, s.max_density, s.avg_speed, s.max_speed, s.force_x, s.force_y,
+                     s.force_z, s.max_stress, bool(s.has_nan), bool(s.valid), s.total_mass, tuple(s.force_sum),
+                     int(s.fluid_cells), {"density_sum": s.density_sum, "speed_sum": s.speed_sum})
+
+    def ProbeSliceHealth(self, zLayer: int) -> bool:
+        d = ctypes.c_int32()
+        self._check(self._lib.fc_lbm_probe_slice_health(self._h, int(zLayer), ctypes.byref(d)), "ProbeSliceHealth")
+        return bool(d.value)
+
+    def HasDiverged(self) -> bool:
+        d = ctypes.c_int32()
+        self._check(self._lib.fc_lbm_has_diverged(self._h, ctypes.byref(d)), "HasDiverged")
+        return bool(d.value)
+
+    def SavePopulations(self) -> np.ndarray:
+        q = 19 if self._model == LatticeModel.D3Q19 else 15
+        out = np.empty(q * self.CellCount(), dtype=np.float32)
+        self._check(self._lib.fc_lbm_save_populations(self._h, out.ctypes.data_as(_FP), out.size), "SavePopulations")
+        return out.reshape(q, self.CellCount())
+
+    def LoadPopulations(self, pops: np.ndarray) -> None:
+        p = np.ascontiguousarray(np.asarray(pops, dtype=np.float32).ravel())
+        self._check(self._lib.fc_lbm_load_populations(self._h, p.ctypes.data_as(_FP), p.size), "LoadPopulations")
+
+    # -- queries ---------------------------------------------------------
+    def SolidMask(self) -> np.ndarray:
+        return self._solid_cpu
+
+    def IsValid(self) -> bool:
+        return bool(self._lib.fc_lbm_is_valid(self._h))
+
+    def Model(self) -> LatticeModel:
+        return self._model
+
+    def _dims(self):
+        x, y, z = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        self._lib.fc_lbm_dims(self._h, ctypes.byref(x), ctypes.byref(y), ctypes.byref(z))
+        return x.value, y.value, z.value
+
+    def Nx(self) -> int:
+        return self._dims()[0]
+
+    def Ny(self) -> int:
+        return self._dims()[1]
+
+    def Nz(self) -> int:
+        return self._dims()[2]
+
+    def CellCount(self) -> int:
+        x, y, z = self._dims()
+        return x * y * z
+
+    def Stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self._lib.fc_lbm_get_stream(self._h, ctypes.byref(s)), "get_stream")
+        return s.value or 0
+
+    def BoundaryInfo(self) -> dict:
+        a, b, c = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        self._lib.fc_lbm_boundary_info(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        return {"boundary_cells": a.value, "bouzidi_links": b.value, "bulk_cells": c.value}
+
+    def StepTimed(self, n: int) -> dict:
+        """n substeps on the solver's stream with CUDA events around every
+        launch: device ms of the sequence and of the bulk / boundary kernels."""
+        t, b, d = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        self._check(self._lib.fc_lbm_step_timed(self._h, int(n), ctypes.byref(t), ctypes.byref(b), ctypes.byref(d)),
+                    "StepTimed")
+        return {"total_ms": t.value, "bulk_ms": b.value, "boundary_ms": d.value}
+
+    def LaunchCount(self) -> int:
+        v = ctypes.c_uint64()
+        self._lib.fc_lbm_launch_count(self._h, ctypes.byref(v))
+        return v.value

@@ -1,0 +1,216 @@
+/*
+ * fc_lbm.h — C ABI of the B200 Lattice-Boltzmann solver (libfc_lbm.so).
+ *
+ * Drop-in replacement for the SDL_GPU compute backend of FlowCraft's
+ * `LbmSolver` (FlowCraft/LbmSolver.h:59-230). Each entry point names the
+ * reference method it replaces. Differences from the reference interface:
+ *   - the SDL_GPUDevice becomes a CUDA device ordinal (fc_lbm_options);
+ *   - the SDL_GPUCommandBuffer argument of Step/StepRange becomes a
+ *     cudaStream_t passed as `void*` (NULL = the solver's own stream);
+ *   - every call returns an int status (FC_LBM_OK or a negative FC_LBM_ERR_*)
+ *     instead of bool/void, and no C++ exception crosses this boundary.
+ *     fc_lbm_last_error() keeps the reference's LastError() string.
+ *
+ * Plain pointers and sizes only: no CUDA, torch or C++ types appear in the
+ * signatures. The handle is not thread-safe (the reference serialises every
+ * call on one mutex, FlowCraft/main.cpp:366-368); one handle, one stream.
+ *
+ * Data layout seen by callers (identical to the reference):
+ *   cell index  = (z*ny + y)*nx + x,
+ *   field       = 4 floats per cell: (rho, ux, uy, uz) at fluid cells,
+ *                 (stress, Fx, Fy, Fz) at solid cells
+ *                 (FlowCraft/LbmReference.cpp:475-500).
+ */
+#ifndef FC_LBM_H
+#define FC_LBM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FC_LBM_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define FC_LBM_API __attribute__((visibility("default")))
+#else
+#define FC_LBM_API
+#endif
+
+/* Status codes. */
+#define FC_LBM_OK 0
+#define FC_LBM_ERR_INVALID_ARG (-1)
+#define FC_LBM_ERR_OUT_OF_MEMORY (-2)
+#define FC_LBM_ERR_CUDA (-3)
+#define FC_LBM_ERR_TIMEOUT (-4)
+#define FC_LBM_ERR_NOT_INITIALIZED (-5)
+#define FC_LBM_ERR_UNSUPPORTED (-6)
+
+/* LatticeModel, same enumerator order as FlowCraft/LatticeModel.h:12. */
+#define FC_LATTICE_D3Q15 0
+#define FC_LATTICE_D3Q19 1
+
+/* Population storage in HBM. FP32 reproduces LbmReference bit-for-bit;
+ * the 16-bit formats store (f_i - w_i) * 2^8 and collide in FP32. */
+#define FC_STORAGE_FP32 0
+#define FC_STORAGE_FP16_OFFSET 1
+#define FC_STORAGE_BF16_OFFSET 2
+
+/* Streaming scheme. PINGPONG keeps two population copies (pull scheme, the
+ * reference's layout); AA keeps one copy updated in place. */
+#define FC_STREAMING_PINGPONG 0
+#define FC_STREAMING_AA 1
+
+/* Where the pointers in fc_grid_desc live. */
+#define FC_MEMORY_HOST 0
+#define FC_MEMORY_DEVICE 1
+
+/* Geometry input: FlowCraft's VoxelGrid (FlowCraft/VoxelGrid.h:13-61).
+ * `solid` holds nx*ny*nz bytes (nonzero = solid). `signed_distance` holds
+ * nx*ny*nz floats (positive in fluid, negative in solid, +-inf far from the
+ * surface) or is NULL, in which case every wall link uses plain halfway
+ * bounce-back (the reference's behaviour for a missing or mis-sized SDF,
+ * LbmReference.cpp:162-166). The solver copies both arrays; neither is
+ * retained. */
+typedef struct fc_grid_desc {
+    int32_t nx, ny, nz;
+    float cell_size;
+    float origin[3];
+    const uint8_t* solid;
+    const float* signed_distance;
+    int32_t memory; /* FC_MEMORY_HOST or FC_MEMORY_DEVICE */
+} fc_grid_desc;
+
+/* LbmSolver::Params (FlowCraft/LbmSolver.h:61-100); the defaults there are
+ * tau 0.8, inlet 0.05, reverse 0, free-slip Y/Z 1, Cs 0.12. */
+typedef struct fc_params {
+    float tau;
+    float inlet_velocity;
+    int32_t reverse_flow;
+    int32_t free_slip_y;
+    int32_t free_slip_z;
+    float smagorinsky_cs;
+} fc_params;
+
+typedef struct fc_options {
+    int32_t device;    /* CUDA device ordinal */
+    int32_t storage;   /* FC_STORAGE_* */
+    int32_t streaming; /* FC_STREAMING_* */
+    int32_t reserved;
+} fc_options;
+
+/* LbmSolver::Stats (FlowCraft/LbmSolver.h:172-184) plus the FP64 sums the
+ * device reduction produces (LbmReference::ComputeStats,
+ * LbmReference.cpp:502-585, also reports total mass). */
+typedef struct fc_stats {
+    float avg_density, min_density, max_density;
+    float avg_speed, max_speed;
+    float force_x, force_y, force_z;
+    float max_stress;
+    int32_t has_nan;
+    int32_t valid;
+    double total_mass;
+    double force_sum[3];
+    double density_sum;
+    double speed_sum;
+    uint64_t fluid_cells;
+} fc_stats;
+
+typedef struct fc_lbm fc_lbm;
+
+/* Allocates an empty solver object (no device work). Pair with destroy. */
+FC_LBM_API int fc_lbm_create(fc_lbm** out);
+/* Releases everything, including the object. NULL is accepted. */
+FC_LBM_API void fc_lbm_destroy(fc_lbm* h);
+
+/* LbmSolver::Init (LbmSolver.cpp:205-366). model: FC_LATTICE_*. opts may be
+ * NULL (device 0, FP32, ping-pong). On failure every device resource is
+ * released and fc_lbm_last_error() says why. */
+FC_LBM_API int fc_lbm_init(fc_lbm* h, const fc_grid_desc* grid, int32_t model, const fc_options* opts);
+/* LbmSolver::Shutdown (LbmSolver.cpp:368-387). The object stays reusable. */
+FC_LBM_API int fc_lbm_shutdown(fc_lbm* h);
+/* LbmSolver::LastError (LbmSolver.h:110). Never NULL. */
+FC_LBM_API const char* fc_lbm_last_error(const fc_lbm* h);
+
+/* LbmSolver::Reset (LbmSolver.cpp:389-427): stores params, seeds every cell
+ * with the uniform equilibrium (quiescent, or the mid-speed seed). */
+FC_LBM_API int fc_lbm_reset(fc_lbm* h, const fc_params* params, int32_t seed_at_mid_speed);
+/* LbmSolver::ResetFromField (LbmSolver.cpp:429-472): per-cell equilibrium
+ * from a 4-float-per-cell field. count must be 4*nx*ny*nz floats; a
+ * mismatch returns FC_LBM_ERR_INVALID_ARG and leaves the state untouched
+ * (the reference silently ignores it, LbmSolver.cpp:430). */
+FC_LBM_API int fc_lbm_reset_from_field(fc_lbm* h, const float* field, size_t count);
+/* LbmSolver::SetParams (LbmSolver.h:135): live, no state change. Rejects a
+ * non-finite value, tau <= 0.5 or Cs < 0 with FC_LBM_ERR_INVALID_ARG. */
+FC_LBM_API int fc_lbm_set_params(fc_lbm* h, const fc_params* params);
+FC_LBM_API int fc_lbm_get_params(const fc_lbm* h, fc_params* out);
+
+/* LbmSolver::Step (LbmSolver.cpp:556-562): n full substeps, enqueued on
+ * `stream` (cudaStream_t; NULL = the solver's own stream). Asynchronous. */
+FC_LBM_API int fc_lbm_step(fc_lbm* h, void* stream, int32_t n);
+/* LbmSolver::StepRange (LbmSolver.cpp:543-554): one substep restricted to
+ * z in [z_start, z_start + z_count); call fc_lbm_advance_substep once after
+ * chunks covering the full z range. */
+FC_LBM_API int fc_lbm_step_range(fc_lbm* h, void* stream, int32_t z_start, int32_t z_count);
+/* LbmSolver::AdvanceSubstep (LbmSolver.h:170). */
+FC_LBM_API int fc_lbm_advance_substep(fc_lbm* h);
+
+/* LbmSolver::ReadbackField (LbmSolver.cpp:722-737). Blocking. `out` holds
+ * count = 4*nx*ny*nz floats. */
+FC_LBM_API int fc_lbm_readback_field(fc_lbm* h, float* out, size_t count);
+/* LbmSolver::ReadbackFieldRange (LbmSolver.cpp:584-651): writes z-layers
+ * [z_start, z_start+z_count) into their slots of a full-size (4*N) array. */
+FC_LBM_API int fc_lbm_readback_field_range(fc_lbm* h, int32_t z_start, int32_t z_count, float* out, size_t count);
+/* LbmSolver::ReadbackStats (LbmSolver.cpp:739-788), reduced on the device
+ * with FP64 accumulators; only the stats struct crosses to the host. */
+FC_LBM_API int fc_lbm_readback_stats(fc_lbm* h, fc_stats* out);
+/* LbmSolver::ProbeSliceHealth (LbmSolver.cpp:653-720): *diverged = 1 when
+ * any cell of layer z (clamped) is non-finite, or a fluid cell has rho <= 0
+ * or |u|^2 > 4. */
+FC_LBM_API int fc_lbm_probe_slice_health(fc_lbm* h, int32_t z, int32_t* diverged);
+/* LbmReference::HasDiverged (LbmReference.h:129): sticky device flag set by
+ * the step kernels for any streamed fluid cell that goes non-finite,
+ * rho <= 0 or |u|^2 > 4; cleared by reset. Waits for queued work. */
+FC_LBM_API int fc_lbm_has_diverged(fc_lbm* h, int32_t* diverged);
+
+/* LbmSolver::SolidMask (LbmSolver.h:224): copies the solver's nx*ny*nz
+ * solid bytes into `out`. */
+FC_LBM_API int fc_lbm_copy_solid_mask(const fc_lbm* h, uint8_t* out, size_t count);
+/* LbmSolver::IsValid / Model / Nx / Ny / Nz (LbmSolver.h:226-230). */
+FC_LBM_API int fc_lbm_is_valid(const fc_lbm* h);
+FC_LBM_API int fc_lbm_model(const fc_lbm* h);
+FC_LBM_API int fc_lbm_dims(const fc_lbm* h, int32_t* nx, int32_t* ny, int32_t* nz);
+
+/* Waits up to timeout_ms (< 0 = forever) for the solver's queued work;
+ * FC_LBM_ERR_TIMEOUT if it is still running. Polls, never spins on the GPU. */
+FC_LBM_API int fc_lbm_sync(fc_lbm* h, int32_t timeout_ms);
+/* The solver's own stream (a cudaStream_t), for callers that order work
+ * against it. */
+FC_LBM_API int fc_lbm_get_stream(const fc_lbm* h, void** stream);
+/* Number of cells handled by the boundary-list kernel and of interpolated
+ * (Bouzidi) links; diagnostics for tests and the bench. */
+FC_LBM_API int fc_lbm_boundary_info(const fc_lbm* h, uint64_t* boundary_cells, uint64_t* bouzidi_links, uint64_t* bulk_cells);
+/* Runs n full substeps on the solver's own stream with CUDA events around
+ * every kernel launch, waits, and reports the device time of the whole
+ * sequence and the summed durations of the bulk and boundary-list kernels
+ * (ms). Measurement aid for benchmarks; results equal fc_lbm_step's. */
+FC_LBM_API int fc_lbm_step_timed(fc_lbm* h, int32_t n, float* total_ms, float* bulk_ms, float* boundary_ms);
+/* Kernel launches this handle has enqueued since init (bench accounting). */
+FC_LBM_API int fc_lbm_launch_count(const fc_lbm* h, uint64_t* launches);
+
+/* Raw populations of the current state in the reference's natural layout
+ * (post-collision, f[i*N + cell]) decoded to FP32: Q*N floats. Solid cells
+ * read back as the reference holds them (the seed before the first step,
+ * w_i after it) although the step never streams them. For checkpoints and
+ * exhaustive tests. */
+FC_LBM_API int fc_lbm_save_populations(fc_lbm* h, float* out, size_t count);
+/* Restores a state written by fc_lbm_save_populations (Q*N floats). */
+FC_LBM_API int fc_lbm_load_populations(fc_lbm* h, const float* in, size_t count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FC_LBM_H */

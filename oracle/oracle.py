@@ -1,0 +1,208 @@
+"""ORACLE — test infrastructure only (tests/, __graft_entry__.smoke(), and the
+CPU-baseline leg of bench.py). The product library never imports this module.
+
+ctypes bindings for the CPU oracle libraries built by ``oracle/Makefile``:
+
+* ``Oracle(precision="f32")`` — the restated algorithm (``lbm_oracle.c``) in
+  float, IEEE op-for-op with FlowCraft's ``LbmReference`` (LbmReference.cpp:241-469);
+* ``Oracle(precision="f64")`` — the same restatement in double, the FP64 error
+  reference;
+* ``Oracle(precision="ref")`` / ``"ref_fast"`` — FlowCraft's own
+  ``LbmReference.cpp`` compiled from its sources (``oracle/_ref/``), when
+  present.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIBS = {
+    "f32": (os.path.join(HERE, "liblbm_oracle32.so"), "oracle32_"),
+    "f64": (os.path.join(HERE, "liblbm_oracle64.so"), "oracle64_"),
+    "ref": (os.path.join(HERE, "_ref", "libfcref.so"), "ref_"),
+    "ref_fast": (os.path.join(HERE, "_ref", "libfcref_fast.so"), "ref_"),
+}
+
+
+class OracleParams(ctypes.Structure):
+    _fields_ = [
+        ("tau", ctypes.c_float),
+        ("inlet_velocity", ctypes.c_float),
+        ("reverse_flow", ctypes.c_int32),
+        ("free_slip_y", ctypes.c_int32),
+        ("free_slip_z", ctypes.c_int32),
+        ("smagorinsky_cs", ctypes.c_float),
+    ]
+
+
+class OracleStats(ctypes.Structure):
+    _fields_ = [
+        ("avg_density", ctypes.c_double),
+        ("min_density", ctypes.c_double),
+        ("max_density", ctypes.c_double),
+        ("avg_speed", ctypes.c_double),
+        ("max_speed", ctypes.c_double),
+        ("force_x", ctypes.c_double),
+        ("force_y", ctypes.c_double),
+        ("force_z", ctypes.c_double),
+        ("max_stress", ctypes.c_double),
+        ("total_mass", ctypes.c_double),
+        ("has_nan", ctypes.c_int32),
+        ("fluid_count_lo", ctypes.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+def build(force: bool = False) -> None:
+    """Compile the oracle libraries (and oracle/_ref when the reference tree exists)."""
+    need = force or not all(os.path.exists(_LIBS[k][0]) for k in ("f32", "f64"))
+    if need or (os.path.isdir("/root/reference") and not os.path.exists(_LIBS["ref"][0])):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def available(precision: str) -> bool:
+    return os.path.exists(_LIBS[precision][0])
+
+
+_loaded: dict = {}
+
+
+def _lib(precision: str):
+    if precision in _loaded:
+        return _loaded[precision]
+    path, prefix = _LIBS[precision]
+    if not os.path.exists(path):
+        if precision in ("f32", "f64"):
+            build()
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle library missing: {path}")
+    lib = ctypes.CDLL(path)
+    vp, c_int, c_size = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t
+    fptr = ctypes.POINTER(ctypes.c_float)
+
+    def fn(name, res, *args):
+        f = getattr(lib, prefix + name)
+        f.restype = res
+        f.argtypes = list(args)
+        return f
+
+    is_ref = prefix == "ref_"
+    create_args = [c_int, c_int, c_int, c_int, ctypes.POINTER(ctypes.c_uint8), fptr, c_size,
+                   ctypes.POINTER(OracleParams), c_int]
+    if not is_ref:
+        create_args.append(c_int)
+    api = {
+        "create": fn("create", vp, *create_args),
+        "destroy": fn("destroy", None, vp),
+        "reset": fn("reset", None, vp, c_int),
+        "reset_from_field": fn("reset_from_field", c_int, vp, fptr, c_size),
+        "set_params": fn("set_params", None, vp, ctypes.POINTER(OracleParams)),
+        "step": fn("step", None, vp, c_int),
+        "has_diverged": fn("has_diverged", c_int, vp),
+        "readback_field": fn("readback_field", None, vp, fptr),
+        "stats": fn("stats", None, vp, ctypes.POINTER(OracleStats)),
+        "is_ref": is_ref,
+    }
+    if not is_ref:
+        api["readback_field_f64"] = fn("readback_field_f64", None, vp, ctypes.POINTER(ctypes.c_double))
+        api["get_populations"] = fn("get_populations", None, vp, fptr, ctypes.POINTER(ctypes.c_double))
+    _loaded[precision] = api
+    return api
+
+
+@dataclass
+class Params:
+    """Mirror of LbmReference::Params (LbmReference.h:41-52), same defaults."""
+    tau: float = 0.8
+    inlet_velocity: float = 0.05
+    reverse_flow: bool = False
+    free_slip_y: bool = True
+    free_slip_z: bool = True
+    smagorinsky_cs: float = 0.12
+
+    def c(self) -> OracleParams:
+        return OracleParams(self.tau, self.inlet_velocity, int(self.reverse_flow), int(self.free_slip_y),
+                            int(self.free_slip_z), self.smagorinsky_cs)
+
+
+class Oracle:
+    """One CPU lattice (restated oracle or the reference build)."""
+
+    def __init__(self, solid: np.ndarray, sdf: np.ndarray | None, q: int, params: Params,
+                 seed_mid: bool = False, precision: str = "f32", threads: int = 0):
+        self.api = _lib(precision)
+        self.precision = precision
+        solid = np.ascontiguousarray(solid, dtype=np.uint8)
+        nz, ny, nx = solid.shape
+        self.shape = (nz, ny, nx)
+        self.q = q
+        self.n = nx * ny * nz
+        self._solid = solid
+        sdf_ptr, sdf_n = None, 0
+        if sdf is not None:
+            self._sdf = np.ascontiguousarray(sdf, dtype=np.float32)
+            sdf_ptr = self._sdf.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+            sdf_n = self._sdf.size
+        p = params.c()
+        args = [nx, ny, nz, q, solid.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), sdf_ptr, sdf_n,
+                ctypes.byref(p), int(seed_mid)]
+        if not self.api["is_ref"]:
+            args.append(threads)
+        self.h = self.api["create"](*args)
+        if not self.h:
+            raise RuntimeError("oracle create failed")
+
+    def close(self):
+        if self.h:
+            self.api["destroy"](self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reset(self, seed_mid: bool = False):
+        self.api["reset"](self.h, int(seed_mid))
+
+    def reset_from_field(self, field: np.ndarray) -> int:
+        field = np.ascontiguousarray(field, dtype=np.float32).ravel()
+        return self.api["reset_from_field"](self.h, field.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), field.size)
+
+    def set_params(self, params: Params):
+        p = params.c()
+        self.api["set_params"](self.h, ctypes.byref(p))
+
+    def step(self, n: int = 1):
+        self.api["step"](self.h, n)
+
+    def has_diverged(self) -> bool:
+        return bool(self.api["has_diverged"](self.h))
+
+    def readback_field(self) -> np.ndarray:
+        out = np.empty(self.n * 4, dtype=np.float32)
+        self.api["readback_field"](self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+        return out
+
+    def readback_field_f64(self) -> np.ndarray:
+        out = np.empty(self.n * 4, dtype=np.float64)
+        self.api["readback_field_f64"](self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return out
+
+    def populations(self) -> np.ndarray:
+        out = np.empty(self.q * self.n, dtype=np.float32)
+        self.api["get_populations"](self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), None)
+        return out.reshape(self.q, self.n)
+
+    def stats(self) -> dict:
+        s = OracleStats()
+        self.api["stats"](self.h, ctypes.byref(s))
+        return s.as_dict()

@@ -1,0 +1,106 @@
+// ORACLE — test infrastructure only. A C-callable shim over FlowCraft's own
+// CPU solver class LbmReference (FlowCraft/LbmReference.h:39-181), compiled
+// together with the reference's unmodified FlowCraft/LbmReference.cpp by
+// oracle/Makefile into oracle/_ref/. It exposes the same entry points as the
+// restated oracle (lbm_oracle.c) so tests can run either against the same
+// inputs; it is used to pin the restatement and to generate golden fixtures,
+// and as the CPU baseline that bench.py times.
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "LbmReference.h"
+
+extern "C" {
+
+struct oracle_params {
+    float tau;
+    float inlet_velocity;
+    int32_t reverse_flow;
+    int32_t free_slip_y;
+    int32_t free_slip_z;
+    float smagorinsky_cs;
+};
+
+struct oracle_stats {
+    double avg_density, min_density, max_density;
+    double avg_speed, max_speed;
+    double force_x, force_y, force_z;
+    double max_stress;
+    double total_mass;
+    int32_t has_nan;
+    int32_t fluid_count_lo;
+};
+
+struct ref_lbm {
+    LbmReference solver;
+    size_t cells = 0;
+};
+
+static LbmReference::Params to_params(const oracle_params* p) {
+    LbmReference::Params r;
+    r.tau = p->tau;
+    r.inletVelocity = p->inlet_velocity;
+    r.reverseFlow = p->reverse_flow != 0;
+    r.freeSlipY = p->free_slip_y != 0;
+    r.freeSlipZ = p->free_slip_z != 0;
+    r.smagorinskyCs = p->smagorinsky_cs;
+    return r;
+}
+
+ref_lbm* ref_create(int nx, int ny, int nz, int q, const uint8_t* solid, const float* sdf, size_t sdf_count,
+                    const oracle_params* p, int seed_mid) {
+    if (nx <= 0 || ny <= 0 || nz <= 0 || (q != 19 && q != 15)) return nullptr;
+    VoxelGrid grid;
+    grid.nx = nx;
+    grid.ny = ny;
+    grid.nz = nz;
+    grid.cellSize = 1.0f;
+    grid.solid.assign(solid, solid + grid.CellCount());
+    if (sdf && sdf_count > 0) grid.signedDistance.assign(sdf, sdf + sdf_count);
+    ref_lbm* r = new ref_lbm();
+    r->cells = grid.CellCount();
+    r->solver.Init(grid, q == 19 ? LatticeModel::D3Q19 : LatticeModel::D3Q15, to_params(p), seed_mid != 0);
+    return r;
+}
+
+void ref_destroy(ref_lbm* r) { delete r; }
+
+void ref_reset(ref_lbm* r, int seed_mid) { r->solver.Reset(seed_mid != 0); }
+
+int ref_reset_from_field(ref_lbm* r, const float* field, size_t count) {
+    std::vector<float> v(field, field + count);
+    r->solver.ResetFromField(v);
+    return count == r->cells * 4 ? 0 : -1;
+}
+
+void ref_set_params(ref_lbm* r, const oracle_params* p) { r->solver.SetParams(to_params(p)); }
+
+void ref_step(ref_lbm* r, int n) {
+    for (int i = 0; i < n; ++i) r->solver.Step();
+}
+
+int ref_has_diverged(const ref_lbm* r) { return r->solver.HasDiverged() ? 1 : 0; }
+
+void ref_readback_field(ref_lbm* r, float* out) {
+    std::vector<float> f = r->solver.ReadbackField();
+    std::memcpy(out, f.data(), f.size() * sizeof(float));
+}
+
+void ref_stats(ref_lbm* r, oracle_stats* s) {
+    LbmReference::Stats st = r->solver.ComputeStats();
+    std::memset(s, 0, sizeof(*s));
+    s->avg_density = st.avgDensity;
+    s->min_density = st.minDensity;
+    s->max_density = st.maxDensity;
+    s->avg_speed = st.avgSpeed;
+    s->max_speed = st.maxSpeed;
+    s->force_x = st.forceX;
+    s->force_y = st.forceY;
+    s->force_z = st.forceZ;
+    s->max_stress = st.maxStress;
+    s->total_mass = st.totalMass;
+    s->has_nan = st.hasNaN ? 1 : 0;
+}
+
+}  // extern "C"
