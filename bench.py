@@ -358,7 +358,7 @@ def run_ours(args, cfg, rank, world, local_rank):
         "bound": "hbm", "achieved": head["bulk_gbs"], "peak": peak, "unit": "GB/s",
         "frac": head["bulk_gbs"] / peak if head["bulk_gbs"] else None,
         "traffic": trf * head["bulk_cells"] if trf else None,
-        "kernel": f"k_bulk_pull<19,{head['variant']}>",
+        "kernel": f"k_bulk_interior<19,{head['variant']}> + k_bulk_shell (all bulk-mask cells)",
         "algorithmic_bytes_per_launch": head["bulk_bytes_per_launch"],
         "peak_source": f"{peak_src} ({'MEASURED_PEAKS.json hbm_gbs' if peak_src == 'measured' else 'fallback'})",
     }

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/fc_lbm.h"
+#include "lattice.cuh"
 #include "lbm_internal.h"
 
 using fc::Geom;
@@ -140,6 +141,24 @@ fc::StepParams step_params(const fc_lbm* h) {
     s.inlet_ux = s.reverse ? -p.inlet_velocity : p.inlet_velocity;
     s.slip_y = p.free_slip_y != 0;
     s.slip_z = p.free_slip_z != 0;
+    // Equilibrium(dir, rho = 1, ux = inlet_ux, 0, 0) as LbmReference.cpp:9-13
+    // computes it (host code is built without FMA contraction).
+    for (int i = 0; i < 19; ++i) s.feq_inlet[i] = 0.0f;
+    for (int i = 0; i < h->q; ++i) {
+        int ex, ey, ez;
+        float w;
+        if (h->q == 19) {
+            ex = fc::Lattice<19>::ex(i), ey = fc::Lattice<19>::ey(i), ez = fc::Lattice<19>::ez(i);
+            w = fc::Lattice<19>::w(i);
+        } else {
+            ex = fc::Lattice<15>::ex(i), ey = fc::Lattice<15>::ey(i), ez = fc::Lattice<15>::ez(i);
+            w = fc::Lattice<15>::w(i);
+        }
+        const float rho = 1.0f, ux = s.inlet_ux, uy = 0.0f, uz = 0.0f;
+        const float eu = (float)ex * ux + (float)ey * uy + (float)ez * uz;
+        const float u2 = ux * ux + uy * uy + uz * uz;
+        s.feq_inlet[i] = w * rho * (1.0f + 3.0f * eu + 4.5f * eu * eu - 1.5f * u2);
+    }
     return s;
 }
 
@@ -295,10 +314,11 @@ int step_range_on(fc_lbm* h, cudaStream_t s, int z0, int zc) {
     const void* fin = h->pop[h->cur];
     void* fout = h->pop[1 - h->cur];
     if (h->n_bulk > 0) {
+        int nl = 0;
         FC_TRY(h, fc::launch_bulk_pull(h->q, h->storage, fin, fout, h->d_bulk_bits, h->g, p, z0, z1 - z0,
-                                       h->d_diverged, s),
+                                       h->d_diverged, s, &nl),
                "bulk step");
-        h->launches++;
+        h->launches += nl;
     }
     const uint32_t b = h->z_begin[(size_t)z0], e = h->z_begin[(size_t)z1];
     if (e > b) {
@@ -723,9 +743,10 @@ int fc_lbm_step_timed(fc_lbm* h, int32_t n, float* total_ms, float* bulk_ms, flo
         cudaEventRecord(ev[2 + 4 * k], h->stream);
         cudaError_t ce = cudaSuccess;
         if (h->n_bulk > 0) {
+            int nl = 0;
             ce = fc::launch_bulk_pull(h->q, h->storage, fin, fout, h->d_bulk_bits, h->g, p, 0, h->g.nz, h->d_diverged,
-                                      h->stream);
-            h->launches++;
+                                      h->stream, &nl);
+            h->launches += nl;
         }
         cudaEventRecord(ev[3 + 4 * k], h->stream);
         cudaEventRecord(ev[4 + 4 * k], h->stream);

@@ -25,6 +25,20 @@ struct StepParams {
     int outlet_x;    // nx-1, or 0 when reverse_flow
     int reverse;
     int slip_y, slip_z;
+    // Inlet equilibrium feq_i(rho = 1, u = (inlet_ux, 0, 0)), computed on the
+    // host with the reference's float operations (LbmReference.cpp:9-13).
+    float feq_inlet[19];
+};
+
+// Work plan of the bulk shell kernel for one z range (see lbm_step.cu).
+struct ShellPlan {
+    unsigned long long n_a, n_b, n_c;  // warp items in the three regions
+    int z0;                            // first z of the range (region a)
+    int zi0;                           // first interior z (region c)
+    int nyf, yf[2];                    // Y-face rows
+    int nyi;                           // interior rows per layer (ny - 2)
+    int nzf, zf[2];                    // Z-face layers inside the range
+    int ncend, cend[2];                // end chunks of a row
 };
 
 // Per-link handling codes of a boundary-list cell, 3 bits per direction.
@@ -37,8 +51,7 @@ enum LinkKind : unsigned {
 };
 // Cell class, stored in bits 60..62 of the 64-bit link word.
 enum CellClass : unsigned {
-    kCellFluid = 0,      // fluid cell with at least one non-stream link
-    kCellPlane = 1,      // fluid cell on x = 0 or x = nx-1 (inlet or outlet this step)
+    kCellFluid = 0,      // fluid cell with a solid neighbour
     kCellSolidFill = 2,  // solid cell at x = 1 or x = nx-2 (an outlet's neighbour)
 };
 constexpr int kClassShift = 60;
@@ -53,8 +66,11 @@ struct BoundaryList {
 
 // ---- launchers (defined in the .cu files) ----
 // storage: 0 fp32, 1 fp16 offset, 2 bf16 offset; q: 15 or 19.
+// Bulk cells of z range [z0, z0+zc): interior + shell kernels. *launched
+// receives the number of kernels enqueued (0..2).
 cudaError_t launch_bulk_pull(int q, int storage, const void* fin, void* fout, const uint32_t* bulk_bits,
-                             const Geom& g, const StepParams& p, int z0, int zc, int* diverged, cudaStream_t s);
+                             const Geom& g, const StepParams& p, int z0, int zc, int* diverged, cudaStream_t s,
+                             int* launched);
 cudaError_t launch_boundary_pull(int q, int storage, const void* fin, void* fout, const BoundaryList& bl,
                                  uint32_t begin, uint32_t end, const Geom& g, const StepParams& p, int* diverged,
                                  cudaStream_t s);

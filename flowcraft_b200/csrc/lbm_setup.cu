@@ -1,6 +1,7 @@
 // Init-time geometry work, all on the device:
-//   * classify every cell: bulk fluid (bit set in the bulk mask) or a
-//     boundary-list entry (flag byte), from the solid mask alone;
+//   * classify every cell: bulk fluid (bit set in the bulk mask: no solid
+//     neighbour, or on the inlet/outlet planes; Y/Z domain faces included)
+//     or a boundary-list entry (flag byte), from the solid mask alone;
 //   * compact the flagged cells into a sorted list (CUB select);
 //   * per list entry, resolve each link: plain pull, halfway bounce-back,
 //     Bouzidi near/far with precomputed coefficients, or domain edge. The
@@ -42,15 +43,17 @@ __global__ void __launch_bounds__(256) k_classify(const uint8_t* __restrict__ so
         if (solid[c]) {
             flag = (x == 1 || x == g.nx - 2);  // a possible outlet neighbour
         } else if (x == 0 || x == g.nx - 1) {
-            flag = true;
+            bulk = true;  // inlet / outlet plane: handled inside the bulk kernel
         } else {
-            bool special = false;
+            // A solid upstream neighbour sends the cell to the list; a
+            // neighbour off the Y/Z edge does not (the bulk kernel mirrors it).
+            bool wall = false;
             for (int i = 1; i < Q; ++i) {
                 const int px = x - L::ex(i), py = y - L::ey(i), pz = z - L::ez(i);
-                if (!in_bounds(g, px, py, pz) || solid[cell_index(g, px, py, pz)]) special = true;
+                if (in_bounds(g, px, py, pz) && solid[cell_index(g, px, py, pz)]) wall = true;
             }
-            flag = special;
-            bulk = !special;
+            flag = wall;
+            bulk = !wall;
         }
         flags[c] = flag ? 1 : 0;
     }
@@ -109,8 +112,6 @@ __global__ void __launch_bounds__(128) k_links(const uint32_t* __restrict__ cell
     uint32_t nb = 0;
     if (solid[c]) {
         word = (unsigned long long)kCellSolidFill << kClassShift;
-    } else if (x == 0 || x == g.nx - 1) {
-        word = (unsigned long long)kCellPlane << kClassShift;
     } else {
         uint32_t co = coef ? coef_off[e] : 0;
         for (int i = 0; i < Q; ++i) {

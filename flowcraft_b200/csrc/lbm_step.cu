@@ -3,18 +3,20 @@
 // twin shaders/lbm_step.comp.glsl:98-364), split into two kernels so the
 // kernel that touches >99% of the cells never branches on geometry:
 //
-//   k_bulk_pull      one thread per cell, warps on 32 consecutive x of one
-//                    row; a warp reads one 32-bit word of the bit-packed bulk
+//   k_bulk_interior  one thread per cell, warps on 32 consecutive x of one
+//   k_bulk_shell     row; a warp reads one 32-bit word of the bit-packed bulk
 //                    mask and every set lane gathers Q populations from its
 //                    upstream neighbours (coalesced SoA loads, the +-x shifts
 //                    misaligned by one element), collides, and writes Q
-//                    populations. Boundary and solid lanes just exit.
+//                    populations. Boundary and solid lanes just exit. The
+//                    shell kernel covers the warps that can hold a Y/Z-face
+//                    cell (mirror / bounce-back sources) or an inlet/outlet
+//                    cell; the interior kernel is a pure pull.
 //   k_boundary_pull  one thread per entry of the compacted boundary list:
-//                    fluid cells with a wall, domain-edge or Bouzidi link,
-//                    the x = 0 / x = nx-1 inlet/outlet planes, and the solid
-//                    cells an outlet may read. Link kinds and Bouzidi
-//                    coefficients were precomputed at init from the solid
-//                    mask and SDF with the reference's float operations.
+//                    fluid cells with a solid neighbour (halfway or Bouzidi
+//                    links) and the solid cells an outlet may read. Link kinds and
+//                    Bouzidi coefficients were precomputed at init from the
+//                    solid mask and SDF with the reference's float operations.
 //
 // Both kernels read one population set and write the other (ping-pong), so
 // they are independent and touch disjoint cells.
@@ -31,32 +33,220 @@ __device__ __forceinline__ long long link_offset(int i, const Geom& g) {
     return (long long)Lattice<Q>::ex(i) + (long long)Lattice<Q>::ey(i) * g.nx + (long long)Lattice<Q>::ez(i) * g.nxy;
 }
 
-template <int Q, class S>
-__global__ void __launch_bounds__(32 * kBulkRows) k_bulk_pull(const typename S::T* __restrict__ fin,
-                                                               typename S::T* __restrict__ fout,
-                                                               const uint32_t* __restrict__ bulk_bits, Geom g,
-                                                               StepParams p, int z0, int* __restrict__ diverged) {
-    const int x = blockIdx.x * 32 + threadIdx.x;
-    const int y = blockIdx.y * kBulkRows + threadIdx.y;
-    const int z = z0 + blockIdx.z;
-    if (y >= g.ny) return;
-    const size_t row = (size_t)z * g.ny + y;
-    const uint32_t bits = __ldg(bulk_bits + row * g.wpr + blockIdx.x);
-    if (!((bits >> threadIdx.x) & 1u)) return;  // bits beyond nx are zero
-    const size_t c = row * g.nx + x;
-
-    float f[Q];
-    static_for<0, Q>([&](auto I) {
-        constexpr int i = decltype(I)::value;
-        f[i] = load_pop_c<Q, S, i>(fin, g.n, c - link_offset<Q>(i, g));
-    });
-    if (collide_regularized<Q>(f, p.tau, p.cs)) atomicOr(diverged, 1);
-    static_for<0, Q>([&](auto I) {
-        constexpr int i = decltype(I)::value;
-        store_pop_c<Q, S, i>(fout, g.n, c, f[i]);
-    });
+// Source of population i for a fluid cell whose upstream neighbour is off
+// the Y and/or Z edge (oy / oz): the free-slip mirror when every wall crossed
+// is free-slip, else plain bounce-back (LbmReference.cpp:370-380). Returns the
+// plane to read at the cell itself; every candidate has the weight of i.
+template <int Q, int I>
+__device__ __forceinline__ int edge_plane(bool oy, bool oz, const StepParams& p) {
+    const bool mirror = (!oy || p.slip_y) && (!oz || p.slip_z);
+    if (!mirror) return Lattice<Q>::opp(I);
+    if (oy && oz) return mirror_z<Q>(mirror_y<Q>(I));
+    return oy ? mirror_y<Q>(I) : mirror_z<Q>(I);
 }
 
+template <int Q, class S>
+__device__ __forceinline__ float load_plane(const typename S::T* __restrict__ f, int plane, size_t n, size_t cell,
+                                            float w) {
+    return S::dec(S::ld(f + (size_t)plane * n + cell), w);
+}
+
+// One bulk cell. General = false is the interior path: a pure pull from the
+// 19 (15) upstream neighbours. General = true adds the Y/Z domain-face
+// sources and the inlet/outlet lanes; it only runs in warps that can hold
+// such cells (face rows, and the first and last warp of each row), so the
+// interior never pays for the selects.
+template <int Q, class S, bool General>
+__device__ __forceinline__ void bulk_cell(const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
+                                          const Geom& g, const StepParams& p, int x, int y, int z, uint32_t c,
+                                          int* __restrict__ diverged) {
+    using L = Lattice<Q>;
+    float f[Q];
+    if constexpr (!General) {
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            f[i] = load_pop_i<Q, S, i>(fin, g.n, c - (uint32_t)link_offset<Q>(i, g));
+        });
+        if (collide<Q, S::kExact>(f, p.tau, p.cs)) atomicOr(diverged, 1);
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            store_pop_i<Q, S, i>(fout, g.n, c, f[i]);
+        });
+    } else {
+        const bool inlet = x == p.inlet_x;
+        const bool outlet = !inlet && x == p.outlet_x;
+        const uint32_t nb = p.reverse ? c + 1u : c - 1u;  // outlet's upstream neighbour (LbmReference.cpp:320)
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            const int py = y - L::ey(i), pz = z - L::ez(i);
+            const bool oy = py < 0 || py >= g.ny;
+            const bool oz = pz < 0 || pz >= g.nz;
+            const bool out = (oy || oz) && !outlet;
+            const int plane = out ? edge_plane<Q, i>(oy, oz, p) : i;
+            // the inlet lane reads nothing; its address is kept in bounds anyway
+            const uint32_t src = outlet ? nb : ((out || inlet) ? c : c - (uint32_t)link_offset<Q>(i, g));
+            f[i] = inlet ? 0.0f : load_plane<Q, S>(fin, plane, g.n, src, L::w(i));
+        });
+        if (outlet) {
+            // zero-gradient outlet: neighbour's fIn moments, rho relaxed
+            // toward 1 (LbmReference.cpp:275-327)
+            float nr, nu, nv, nw;
+            moments<Q>(f, nr, nu, nv, nw);
+            const float rho = nr > 1e-6f ? 1.0f + 0.999f * (nr - 1.0f) : 1.0f;
+            equilibrium_all<Q>(rho, nu, nv, nw, f);
+        } else {
+            const bool bad = collide<Q, S::kExact>(f, p.tau, p.cs);
+            if (bad && !inlet) atomicOr(diverged, 1);
+        }
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            store_pop_i<Q, S, i>(fout, g.n, c, inlet ? p.feq_inlet[i] : f[i]);
+        });
+    }
+}
+
+// The bulk cells (every fluid cell without a solid neighbour, plus the fluid
+// cells of the x = 0 and x = nx-1 planes) are split by warp position into a
+// disjoint interior and shell, each its own kernel so each gets its own
+// register allocation:
+//   interior  rows with 1 <= y <= ny-2 and 1 <= z <= nz-2, 32-cell chunks
+//             1 .. wpr-2 of the row: no face, inlet or outlet cell can occur;
+//   shell     Y-face rows (all chunks), Z-face rows (all chunks), and the
+//             first and last chunk of every other row.
+// Folding the inlet/outlet planes into warps makes their accesses part of
+// coalesced requests instead of one element per 32-byte sector.
+template <int Q, class S>
+__global__ void __launch_bounds__(32 * kBulkRows) k_bulk_interior(const typename S::T* __restrict__ fin,
+                                                                   typename S::T* __restrict__ fout,
+                                                                   const uint32_t* __restrict__ bulk_bits, Geom g,
+                                                                   StepParams p, int z0, int* __restrict__ diverged) {
+    const int chunk = blockIdx.x + 1;
+    const int x = chunk * 32 + threadIdx.x;
+    const int y = 1 + blockIdx.y * kBulkRows + threadIdx.y;
+    const int z = z0 + blockIdx.z;
+    if (y >= g.ny - 1) return;
+    const size_t row = (size_t)z * g.ny + y;
+    const uint32_t bits = __ldg(bulk_bits + row * g.wpr + chunk);
+    if (!((bits >> threadIdx.x) & 1u)) return;
+    const uint32_t c = (uint32_t)(row * g.nx + x);
+    bulk_cell<Q, S, false>(fin, fout, g, p, x, y, z, c, diverged);
+}
+
+// Interior, two x-adjacent cells per thread (lattices with even nx): a warp
+// covers 64 cells of a row starting at x = 32 + 64*blockIdx.x, so every pair
+// starts on an even cell index. The directions with e_x = 0 read both cells
+// of a pair with one aligned 2-element load, every store is one 2-element
+// store, and both cells share each address. Per direction the source pointer
+// fin + i*n - offset_i is the same for every thread, so an access costs one
+// index-times-stride from a uniform base. Pairs with one bulk cell (next to a
+// wall) fall back to the one-cell path for that cell.
+template <int Q, class S>
+__global__ void __launch_bounds__(32 * kBulkRows) k_bulk_interior2(const typename S::T* __restrict__ fin,
+                                                                    typename S::T* __restrict__ fout,
+                                                                    const uint32_t* __restrict__ bulk_bits, Geom g,
+                                                                    StepParams p, int z0, int* __restrict__ diverged) {
+    using L = Lattice<Q>;
+    using T = typename S::T;
+    const int w0 = 1 + 2 * blockIdx.x;  // first 32-cell chunk of this warp's 64 cells
+    const int y = 1 + blockIdx.y * kBulkRows + threadIdx.y;
+    const int z = z0 + blockIdx.z;
+    if (y >= g.ny - 1) return;
+    const size_t row = (size_t)z * g.ny + y;
+    const int k = 2 * threadIdx.x;  // 0..62 within the 64 cells
+    const int w = w0 + (k >> 5);
+    const uint32_t bits = w <= g.wpr - 2 ? __ldg(bulk_bits + row * g.wpr + w) : 0u;
+    const unsigned pair = (bits >> (k & 31)) & 3u;
+    if (!pair) return;
+    const int x = w0 * 32 + k;
+    const uint32_t c = (uint32_t)(row * g.nx + x);
+    if (pair != 3u) {  // only one of the two cells is a bulk cell
+        const uint32_t cc = pair == 1u ? c : c + 1u;
+        bulk_cell<Q, S, false>(fin, fout, g, p, x + (pair == 1u ? 0 : 1), y, z, cc, diverged);
+        return;
+    }
+    float a[Q], b[Q];
+    if constexpr (S::kExact) {
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            const T* src = fin + ((long long)i * (long long)g.n - link_offset<Q>(i, g));
+            if constexpr (L::ex(i) == 0) {
+                const float2 v = S::dec2(S::ld2(src + c), L::w(i));
+                a[i] = v.x;
+                b[i] = v.y;
+            } else {
+                a[i] = S::dec(S::ld(src + c), L::w(i));
+                b[i] = S::dec(S::ld(src + c + 1u), L::w(i));
+            }
+        });
+        const bool bad_a = collide<Q, true>(a, p.tau, p.cs);
+        const bool bad_b = collide<Q, true>(b, p.tau, p.cs);
+        if (bad_a | bad_b) atomicOr(diverged, 1);
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            T* dst = fout + (size_t)i * g.n;
+            *reinterpret_cast<typename S::T2*>(dst + c) = S::enc2(a[i], b[i], L::w(i));
+        });
+    } else {  // 16-bit offsets: collide on the stored representation
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            const T* src = fin + ((long long)i * (long long)g.n - link_offset<Q>(i, g));
+            if constexpr (L::ex(i) == 0) {
+                const float2 v = S::raw2(S::ld2(src + c));
+                a[i] = v.x;
+                b[i] = v.y;
+            } else {
+                a[i] = S::raw(S::ld(src + c));
+                b[i] = S::raw(S::ld(src + c + 1u));
+            }
+        });
+        const bool bad_a = collide_offsets<Q>(a, p.tau, p.cs);
+        const bool bad_b = collide_offsets<Q>(b, p.tau, p.cs);
+        if (bad_a | bad_b) atomicOr(diverged, 1);
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            T* dst = fout + (size_t)i * g.n;
+            *reinterpret_cast<typename S::T2*>(dst + c) = S::pack2(a[i], b[i]);
+        });
+    }
+}
+
+template <int Q, class S>
+__global__ void __launch_bounds__(32 * kBulkRows) k_bulk_shell(const typename S::T* __restrict__ fin,
+                                                                typename S::T* __restrict__ fout,
+                                                                const uint32_t* __restrict__ bulk_bits, Geom g,
+                                                                StepParams p, ShellPlan sp, int* __restrict__ diverged) {
+    // one warp per (row, chunk) item of the shell
+    unsigned long long item = (unsigned long long)blockIdx.x * kBulkRows + threadIdx.y;
+    int chunk, y, z;
+    if (item < sp.n_a) {  // Y-face rows, every chunk
+        chunk = (int)(item % g.wpr);
+        const unsigned long long r = item / g.wpr;
+        y = sp.yf[(int)(r % sp.nyf)];
+        z = sp.z0 + (int)(r / sp.nyf);
+    } else if ((item -= sp.n_a) < sp.n_b) {  // Z-face rows off the Y faces, every chunk
+        chunk = (int)(item % g.wpr);
+        const unsigned long long r = item / g.wpr;
+        y = 1 + (int)(r % sp.nyi);
+        z = sp.zf[(int)(r / sp.nyi)];
+    } else if ((item -= sp.n_b) < sp.n_c) {  // end chunks of interior rows
+        chunk = sp.cend[(int)(item % sp.ncend)];
+        const unsigned long long r = item / sp.ncend;
+        y = 1 + (int)(r % sp.nyi);
+        z = sp.zi0 + (int)(r / sp.nyi);
+    } else {
+        return;
+    }
+    const size_t row = (size_t)z * g.ny + y;
+    const uint32_t bits = __ldg(bulk_bits + row * g.wpr + chunk);
+    if (!((bits >> threadIdx.x) & 1u)) return;
+    const int x = chunk * 32 + threadIdx.x;
+    const uint32_t c = (uint32_t)(row * g.nx + x);
+    bulk_cell<Q, S, true>(fin, fout, g, p, x, y, z, c, diverged);
+}
+
+// Boundary-list entries: fluid cells with a solid neighbour (off the
+// inlet/outlet planes) and the solid cells an outlet reads. Every link's source
+// address is formed with selects first and all loads issue together.
 template <int Q, class S>
 __global__ void __launch_bounds__(128) k_boundary_pull(const typename S::T* __restrict__ fin,
                                                         typename S::T* __restrict__ fout, BoundaryList bl,
@@ -68,10 +258,10 @@ __global__ void __launch_bounds__(128) k_boundary_pull(const typename S::T* __re
     const uint32_t c = __ldg(bl.cells + e);
     const unsigned long long lk = __ldg(bl.links + e);
     const unsigned cls = (unsigned)(lk >> kClassShift) & 7u;
-    const uint32_t z = (uint32_t)(c / (unsigned long long)g.nxy);
-    const uint32_t rem = c - z * (uint32_t)g.nxy;
+    const uint32_t nxy = (uint32_t)g.nxy;
+    const uint32_t z = c / nxy;
+    const uint32_t rem = c - z * nxy;
     const uint32_t y = rem / (uint32_t)g.nx;
-    const int x = (int)(rem - y * (uint32_t)g.nx);
 
     float f[Q];
     if (cls == kCellSolidFill) {  // solid cell: f_i = w_i (LbmReference.cpp:264-267)
@@ -81,68 +271,38 @@ __global__ void __launch_bounds__(128) k_boundary_pull(const typename S::T* __re
         });
         return;
     }
-    if (cls == kCellPlane) {
-        if (x == p.inlet_x) {  // equilibrium at rho = 1, u = (+-U, 0, 0) (LbmReference.cpp:269-273)
-            equilibrium_all<Q>(1.0f, p.inlet_ux, 0.0f, 0.0f, f);
-        } else {  // zero-gradient outlet from the neighbour's fIn moments (LbmReference.cpp:275-327)
-            const size_t nb = p.reverse ? (size_t)c + 1 : (size_t)c - 1;
-            float g0[Q];
-            static_for<0, Q>([&](auto I) {
-                constexpr int i = decltype(I)::value;
-                g0[i] = load_pop_c<Q, S, i>(fin, g.n, nb);
-            });
-            float nr, nu, nv, nw;
-            moments<Q>(g0, nr, nu, nv, nw);
-            const float rho = nr > 1e-6f ? 1.0f + 0.999f * (nr - 1.0f) : 1.0f;
-            equilibrium_all<Q>(rho, nu, nv, nw, f);
-        }
-        static_for<0, Q>([&](auto I) {
-            constexpr int i = decltype(I)::value;
-            store_pop_c<Q, S, i>(fout, g.n, c, f[i]);
-        });
-        return;
-    }
-
-    // Fluid cell next to a wall, an edge, or both (LbmReference.cpp:329-383).
-    uint32_t co = __ldg(bl.coef_off + e);
+    // Fluid cell next to a wall (LbmReference.cpp:329-383).
+    const uint32_t co0 = __ldg(bl.coef_off + e);
+    uint32_t bzmask = 0;  // directions that carry a Bouzidi coefficient pair
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        if ((((unsigned)(lk >> (3 * i))) & 6u) == 2u) bzmask |= 1u << i;
+    });
     static_for<0, Q>([&](auto I) {
         constexpr int i = decltype(I)::value;
         constexpr int op = L::opp(i);
         const unsigned kind = (unsigned)(lk >> (3 * i)) & 7u;
-        float v;
+        int pa = op;
+        size_t sa = c;
         if (kind == kLinkStream) {
-            v = load_pop_c<Q, S, i>(fin, g.n, (size_t)c - link_offset<Q>(i, g));
-        } else if (kind == kLinkBounce) {
-            v = load_pop_c<Q, S, op>(fin, g.n, c);
-        } else if (kind == kLinkBzNear) {
-            const float2 k = __ldg(bl.coef + co++);
-            const float a = load_pop_c<Q, S, op>(fin, g.n, c);
-            const float b = load_pop_c<Q, S, op>(fin, g.n, (size_t)c + link_offset<Q>(i, g));
-            v = k.x * a + k.y * b;
-        } else if (kind == kLinkBzFar) {
-            const float2 k = __ldg(bl.coef + co++);
-            const float a = load_pop_c<Q, S, op>(fin, g.n, c);
-            const float b = load_pop_c<Q, S, i>(fin, g.n, c);
-            v = k.x * a + k.y * b;
-        } else {
-            // Off the Y and/or Z edge: free-slip mirror if every wall crossed
-            // is free-slip, else plain bounce-back (LbmReference.cpp:370-380).
+            pa = i;
+            sa = (size_t)c - link_offset<Q>(i, g);
+        } else if (kind == kLinkEdge) {
             const int py = (int)y - L::ey(i), pz = (int)z - L::ez(i);
-            const bool oy = py < 0 || py >= g.ny;
-            const bool oz = pz < 0 || pz >= g.nz;
-            const bool mirror = (oy || oz) && (!oy || p.slip_y) && (!oz || p.slip_z);
-            if (!mirror)
-                v = load_pop_c<Q, S, op>(fin, g.n, c);
-            else if (oy && oz)
-                v = load_pop_c<Q, S, mirror_z<Q>(mirror_y<Q>(i))>(fin, g.n, c);
-            else if (oy)
-                v = load_pop_c<Q, S, mirror_y<Q>(i)>(fin, g.n, c);
-            else
-                v = load_pop_c<Q, S, mirror_z<Q>(i)>(fin, g.n, c);
+            pa = edge_plane<Q, i>(py < 0 || py >= g.ny, pz < 0 || pz >= g.nz, p);
+        }
+        const float va = load_plane<Q, S>(fin, pa, g.n, sa, L::w(i));
+        float v = va;
+        if (kind == kLinkBzNear || kind == kLinkBzFar) {
+            const float2 k = __ldg(bl.coef + co0 + __popc(bzmask & ((1u << i) - 1u)));
+            const int pb = kind == kLinkBzNear ? op : i;
+            const size_t sb = kind == kLinkBzNear ? (size_t)c + link_offset<Q>(i, g) : (size_t)c;
+            const float vb = load_plane<Q, S>(fin, pb, g.n, sb, L::w(i));
+            v = k.x * va + k.y * vb;
         }
         f[i] = v;
     });
-    if (collide_regularized<Q>(f, p.tau, p.cs)) atomicOr(diverged, 1);
+    if (collide<Q, S::kExact>(f, p.tau, p.cs)) atomicOr(diverged, 1);
     static_for<0, Q>([&](auto I) {
         constexpr int i = decltype(I)::value;
         store_pop_c<Q, S, i>(fout, g.n, c, f[i]);
@@ -151,11 +311,49 @@ __global__ void __launch_bounds__(128) k_boundary_pull(const typename S::T* __re
 
 template <int Q, class S>
 static cudaError_t bulk_t(const void* fin, void* fout, const uint32_t* bits, const Geom& g, const StepParams& p,
-                          int z0, int zc, int* dv, cudaStream_t s) {
+                          int z0, int zc, int* dv, cudaStream_t s, int* launched) {
+    *launched = 0;
     if (zc <= 0) return cudaSuccess;
+    const int z1 = z0 + zc;
     dim3 block(32, kBulkRows, 1);
-    dim3 grid((unsigned)g.wpr, (unsigned)((g.ny + kBulkRows - 1) / kBulkRows), (unsigned)zc);
-    k_bulk_pull<Q, S><<<grid, block, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout, bits, g, p, z0, dv);
+    // interior: chunks 1..wpr-2, rows 1..ny-2, z in [max(z0,1), min(z1,nz-1))
+    const int zi0 = z0 > 1 ? z0 : 1, zi1 = z1 < g.nz - 1 ? z1 : g.nz - 1;
+    if (g.wpr > 2 && g.ny > 2 && zi1 > zi0) {
+        const unsigned gy = (unsigned)((g.ny - 2 + kBulkRows - 1) / kBulkRows);
+        if (g.nx % 2 == 0) {  // pairs start on even cells
+            dim3 grid((unsigned)((g.wpr - 2 + 1) / 2), gy, (unsigned)(zi1 - zi0));
+            k_bulk_interior2<Q, S><<<grid, block, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout, bits, g, p,
+                                                          zi0, dv);
+        } else {
+            dim3 grid((unsigned)(g.wpr - 2), gy, (unsigned)(zi1 - zi0));
+            k_bulk_interior<Q, S><<<grid, block, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout, bits, g, p,
+                                                         zi0, dv);
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        ++*launched;
+    }
+    ShellPlan sp{};
+    sp.z0 = z0;
+    sp.nyf = 0;
+    sp.yf[sp.nyf++] = 0;
+    if (g.ny > 1) sp.yf[sp.nyf++] = g.ny - 1;
+    sp.nyi = g.ny > 2 ? g.ny - 2 : 0;
+    sp.nzf = 0;
+    if (z0 <= 0 && 0 < z1) sp.zf[sp.nzf++] = 0;
+    if (g.nz > 1 && z0 <= g.nz - 1 && g.nz - 1 < z1) sp.zf[sp.nzf++] = g.nz - 1;
+    sp.zi0 = zi0;
+    sp.ncend = 0;
+    sp.cend[sp.ncend++] = 0;
+    if (g.wpr > 1) sp.cend[sp.ncend++] = g.wpr - 1;
+    sp.n_a = (unsigned long long)sp.nyf * zc * g.wpr;
+    sp.n_b = (unsigned long long)sp.nzf * sp.nyi * g.wpr;
+    sp.n_c = zi1 > zi0 ? (unsigned long long)(zi1 - zi0) * sp.nyi * sp.ncend : 0ull;
+    const unsigned long long items = sp.n_a + sp.n_b + sp.n_c;
+    if (items == 0) return cudaSuccess;
+    const unsigned blocks = (unsigned)((items + kBulkRows - 1) / kBulkRows);
+    k_bulk_shell<Q, S><<<blocks, block, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout, bits, g, p, sp, dv);
+    ++*launched;
     return cudaGetLastError();
 }
 
@@ -185,8 +383,9 @@ static cudaError_t boundary_t(const void* fin, void* fout, const BoundaryList& b
     } while (0)
 
 cudaError_t launch_bulk_pull(int q, int storage, const void* fin, void* fout, const uint32_t* bulk_bits,
-                             const Geom& g, const StepParams& p, int z0, int zc, int* diverged, cudaStream_t s) {
-    FC_DISPATCH(q, storage, bulk_t, fin, fout, bulk_bits, g, p, z0, zc, diverged, s);
+                             const Geom& g, const StepParams& p, int z0, int zc, int* diverged, cudaStream_t s,
+                             int* launched) {
+    FC_DISPATCH(q, storage, bulk_t, fin, fout, bulk_bits, g, p, z0, zc, diverged, s, launched);
 }
 
 cudaError_t launch_boundary_pull(int q, int storage, const void* fin, void* fout, const BoundaryList& bl,

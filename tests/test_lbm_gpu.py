@@ -161,31 +161,53 @@ def test_reset_from_field_mismatch_is_ignored(gpu):
     assert np.array_equal(sim.readback_field(), before)
 
 
-def test_divergence_detection_from_host_injected_state(gpu):
-    """Failure detection without a GPU fault: a host-prepared field with a
-    NaN cell and one with negative density are seeded through
-    ResetFromField; the step's device flag and the slice probe report it, and
-    Reset clears it."""
+def test_divergence_detection_from_host_injected_state(gpu, oracle_built):
+    """Failure detection without a GPU fault: host-prepared fields with a NaN
+    cell, and with a 3x3x3 block at negative density, are seeded through
+    ResetFromField; the step's device flag and the slice probe report them
+    exactly when the reference's divergence test (LbmReference.cpp:397-400)
+    does, and Reset clears the flag."""
     case = CASES["sphere48_q19"]
     sim = GpuAdapter(case)
     sim.step(5)
     assert sim.s.HasDiverged() is False
-    field = sim.readback_field().reshape(-1, 4).copy()
+    base = sim.readback_field().reshape(-1, 4).copy()
     nx, ny = 48, 24
-    c = (10 * ny + 3) * nx + 30  # fluid cell at z=10
-    field[c, 0] = np.nan
-    sim.reset_from_field(field.ravel())
+    cell = lambda x, y, z: (z * ny + y) * nx + x  # noqa: E731
+
+    def inject(field):
+        sim.reset_from_field(field.ravel())
+        ora = OracleAdapter(case)
+        ora.reset_from_field(field.ravel())
+        return ora
+
+    f1 = base.copy()
+    f1[cell(30, 3, 10), 0] = np.nan
+    ora = inject(f1)
     assert sim.s.HasDiverged() is False
-    assert sim.s.ProbeSliceHealth(10) is True
+    assert sim.s.ProbeSliceHealth(10) is True and sim.s.ProbeSliceHealth(2) is False
     sim.step(1)
-    assert sim.s.HasDiverged() is True
+    ora.step(1)
+    assert sim.s.HasDiverged() is True and ora.o.has_diverged()
+
     sim.s.Reset(_params(case["params"]), True)
     assert sim.s.HasDiverged() is False
-    field2 = sim.readback_field().reshape(-1, 4).copy()
-    field2[c, 0] = -1.0
-    sim.reset_from_field(field2.ravel())
+    f2 = base.copy()
+    single = f2.copy()
+    single[cell(30, 3, 10), 0] = -1.0  # one cell: its neighbours stay positive
+    ora = inject(single)
     sim.step(1)
-    assert sim.s.HasDiverged() is True
+    ora.step(1)
+    assert sim.s.HasDiverged() is bool(ora.o.has_diverged()) is False
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                f2[cell(30 + dx, 4 + dy, 10 + dz), 0] = -1.0
+    ora = inject(f2)
+    assert sim.s.ProbeSliceHealth(10) is True
+    sim.step(1)
+    ora.step(1)
+    assert sim.s.HasDiverged() is bool(ora.o.has_diverged()) is True
 
 
 def test_wing_cross_check(gpu):
@@ -202,11 +224,13 @@ def test_wing_cross_check(gpu):
     assert abs(s[19].avgSpeed - s[15].avgSpeed) < 0.005
 
 
-@pytest.mark.parametrize("storage,tol_u,tol_rho", [("FP16_OFFSET", 2e-5, 2e-5), ("BF16_OFFSET", 3e-4, 3e-4)])
+@pytest.mark.parametrize("storage,tol_u,tol_rho", [("FP16_OFFSET", 2e-4, 2e-4), ("BF16_OFFSET", 2e-3, 2e-3)])
 def test_offset_storage_error_vs_fp64(gpu, oracle_built, storage, tol_u, tol_rho):
     """16-bit (f_i - w_i)*2^8 storage, FP32 collision: error against the FP64
-    oracle on the reference test case (60 steps). The reference's own GPU
-    check allows 1e-2 for its plain FP16 storage (gpu_vs_cpu_test.cpp:76)."""
+    oracle on the reference test case (60 steps). Per-step rounding of the
+    stored offsets is ~5e-6 (FP16) / ~4e-5 (BF16) per population and adds up
+    like a random walk over the steps. The reference's own GPU check allows
+    1e-2 for its plain FP16 storage (gpu_vs_cpu_test.cpp:76)."""
     from flowcraft_b200.lbm import Storage
     for q in (19, 15):
         case = CASES[f"sphere48_q{q}"]
@@ -219,6 +243,7 @@ def test_offset_storage_error_vs_fp64(gpu, oracle_built, storage, tol_u, tol_rho
         solid = geometry(case["geom"])[0].ravel().astype(bool)
         d = np.abs(g - r)[~solid]
         assert np.isfinite(g).all()
+        print(f"{storage} D3Q{q}: max|drho| {d[:, 0].max():.3e}  max|du| {d[:, 1:].max():.3e}")
         assert d[:, 0].max() < tol_rho, d[:, 0].max()
         assert d[:, 1:].max() < tol_u, d[:, 1:].max()
 
@@ -235,3 +260,55 @@ def test_init_errors(gpu):
     assert np.array_equal(s.SolidMask(), g.solid)
     s.Shutdown()
     assert not s.IsValid()
+
+
+# Lattice shapes that route cells through every bulk-kernel variant: even nx
+# with an odd number of interior 32-cell chunks (the two-cell interior kernel
+# with a half-masked last group), odd nx (the one-cell interior kernel), a
+# single interior chunk, and the shell (faces, inlet/outlet warps).
+SHAPES = [
+    ("even_masked", (160, 40, 40), (52.0, 20.0, 20.0, 7.0), dict(tau=0.56, inlet_velocity=0.06, smagorinsky_cs=0.1)),
+    ("odd", (161, 41, 39), (50.3, 19.7, 20.2, 6.5),
+     dict(tau=0.6, inlet_velocity=0.05, smagorinsky_cs=0.12, free_slip_y=0, reverse_flow=1)),
+    ("one_chunk", (96, 20, 24), (30.0, 10.0, 12.0, 4.5),
+     dict(tau=0.58, inlet_velocity=0.05, smagorinsky_cs=0.12, free_slip_z=0)),
+]
+
+
+def _shape_case(shape, sphere, params, q=19):
+    nx, ny, nz = shape
+    return dict(geom={"kind": "sphere", "dims": [nx, ny, nz], "center": list(sphere[:3]), "r": sphere[3]}, q=q,
+                params=params, seed_mid=True, steps=[40])
+
+
+@pytest.mark.parametrize("name,shape,sphere,params", SHAPES, ids=[s[0] for s in SHAPES])
+@pytest.mark.parametrize("q", [19, 15])
+def test_fp32_bit_exact_all_kernel_variants(gpu, oracle_built, name, shape, sphere, params, q):
+    case = _shape_case(shape, sphere, params, q)
+    sim = GpuAdapter(case)
+    ora = OracleAdapter(case)
+    sim.step(40)
+    ora.step(40)
+    g, r = sim.readback_field(), ora.readback_field()
+    assert np.array_equal(g.view(np.uint32), r.view(np.uint32)), f"{name} D3Q{q}: differs from the oracle"
+    info = sim.s.BoundaryInfo()
+    assert info["bulk_cells"] > 0 and info["boundary_cells"] > 0
+
+
+@pytest.mark.parametrize("storage,tol", [("FP16_OFFSET", 2e-4), ("BF16_OFFSET", 2e-3)])
+def test_offset_storage_two_cell_kernel_vs_fp64(gpu, oracle_built, storage, tol):
+    """The 16-bit formats through the two-cell interior kernel (even nx with
+    interior chunks), against the FP64 oracle."""
+    from flowcraft_b200.lbm import Storage
+    name, shape, sphere, params = SHAPES[0]
+    case = _shape_case(shape, sphere, params)
+    sim = GpuAdapter(case, storage=Storage[storage])
+    ref = OracleAdapter(case, "f64")
+    sim.step(60)
+    ref.step(60)
+    g = sim.readback_field().reshape(-1, 4).astype(np.float64)
+    r = ref.o.readback_field_f64().reshape(-1, 4)
+    solid = geometry(case["geom"])[0].ravel().astype(bool)
+    d = np.abs(g - r)[~solid]
+    print(f"{storage} {shape}: max|drho| {d[:, 0].max():.3e}  max|du| {d[:, 1:].max():.3e}")
+    assert np.isfinite(g).all() and d[:, 0].max() < tol and d[:, 1:].max() < tol
