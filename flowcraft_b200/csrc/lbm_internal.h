@@ -30,6 +30,15 @@ struct StepParams {
     float feq_inlet[19];
 };
 
+// Per-direction plane pointers of one step, computed on the host:
+// src[i] = fin + i*n - (e_x + e_y nx + e_z nx ny) (the upstream neighbour of
+// cell c in plane i is src[i][c]) and dst[i] = fout + i*n. Passing them as
+// kernel parameters leaves one index-times-stride per access in the kernel.
+struct PlanePtrs {
+    const void* src[19];
+    void* dst[19];
+};
+
 // Work plan of the bulk shell kernel for one z range (see lbm_step.cu).
 struct ShellPlan {
     unsigned long long n_a, n_b, n_c;  // warp items in the three regions

@@ -21,6 +21,7 @@
 // Both kernels read one population set and write the other (ping-pong), so
 // they are independent and touch disjoint cells.
 #include "collide.cuh"
+#include "collide2.cuh"
 #include "lbm_internal.h"
 #include "storage.cuh"
 
@@ -144,7 +145,8 @@ template <int Q, class S>
 __global__ void __launch_bounds__(32 * kBulkRows) k_bulk_interior2(const typename S::T* __restrict__ fin,
                                                                     typename S::T* __restrict__ fout,
                                                                     const uint32_t* __restrict__ bulk_bits, Geom g,
-                                                                    StepParams p, int z0, int* __restrict__ diverged) {
+                                                                    StepParams p, PlanePtrs pp, int z0,
+                                                                    int* __restrict__ diverged) {
     using L = Lattice<Q>;
     using T = typename S::T;
     const int w0 = 1 + 2 * blockIdx.x;  // first 32-cell chunk of this warp's 64 cells
@@ -164,50 +166,45 @@ __global__ void __launch_bounds__(32 * kBulkRows) k_bulk_interior2(const typenam
         bulk_cell<Q, S, false>(fin, fout, g, p, x + (pair == 1u ? 0 : 1), y, z, cc, diverged);
         return;
     }
-    float a[Q], b[Q];
-    if constexpr (S::kExact) {
+    // both cells of the pair in one float2 per direction (cell x in .x)
+    float2 v[Q];
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        const T* src = static_cast<const T*>(pp.src[i]);
+        if constexpr (S::kExact) {
+            v[i] = L::ex(i) == 0 ? S::dec2(S::ld2(src + c), L::w(i))
+                                 : make_float2(S::dec(S::ld(src + c), L::w(i)), S::dec(S::ld(src + c + 1u), L::w(i)));
+        } else {  // 16-bit offsets: collide on the stored representation
+            v[i] = L::ex(i) == 0 ? S::raw2(S::ld2(src + c))
+                                 : make_float2(S::raw(S::ld(src + c)), S::raw(S::ld(src + c + 1u)));
+        }
+    });
+    bool bad;
+    if constexpr (S::kExact) {  // bit-exact path: the scalar reference-order collision per cell
+        float a[Q], b[Q];
         static_for<0, Q>([&](auto I) {
             constexpr int i = decltype(I)::value;
-            const T* src = fin + ((long long)i * (long long)g.n - link_offset<Q>(i, g));
-            if constexpr (L::ex(i) == 0) {
-                const float2 v = S::dec2(S::ld2(src + c), L::w(i));
-                a[i] = v.x;
-                b[i] = v.y;
-            } else {
-                a[i] = S::dec(S::ld(src + c), L::w(i));
-                b[i] = S::dec(S::ld(src + c + 1u), L::w(i));
-            }
+            a[i] = v[i].x;
+            b[i] = v[i].y;
         });
-        const bool bad_a = collide<Q, true>(a, p.tau, p.cs);
-        const bool bad_b = collide<Q, true>(b, p.tau, p.cs);
-        if (bad_a | bad_b) atomicOr(diverged, 1);
+        bad = collide_regularized<Q>(a, p.tau, p.cs);
+        bad |= collide_regularized<Q>(b, p.tau, p.cs);
         static_for<0, Q>([&](auto I) {
             constexpr int i = decltype(I)::value;
-            T* dst = fout + (size_t)i * g.n;
-            *reinterpret_cast<typename S::T2*>(dst + c) = S::enc2(a[i], b[i], L::w(i));
+            v[i] = make_float2(a[i], b[i]);
         });
-    } else {  // 16-bit offsets: collide on the stored representation
-        static_for<0, Q>([&](auto I) {
-            constexpr int i = decltype(I)::value;
-            const T* src = fin + ((long long)i * (long long)g.n - link_offset<Q>(i, g));
-            if constexpr (L::ex(i) == 0) {
-                const float2 v = S::raw2(S::ld2(src + c));
-                a[i] = v.x;
-                b[i] = v.y;
-            } else {
-                a[i] = S::raw(S::ld(src + c));
-                b[i] = S::raw(S::ld(src + c + 1u));
-            }
-        });
-        const bool bad_a = collide_offsets<Q>(a, p.tau, p.cs);
-        const bool bad_b = collide_offsets<Q>(b, p.tau, p.cs);
-        if (bad_a | bad_b) atomicOr(diverged, 1);
-        static_for<0, Q>([&](auto I) {
-            constexpr int i = decltype(I)::value;
-            T* dst = fout + (size_t)i * g.n;
-            *reinterpret_cast<typename S::T2*>(dst + c) = S::pack2(a[i], b[i]);
-        });
+    } else {
+        bad = collide_offsets2<Q>(v, p.tau, p.cs);
     }
+    if (bad) atomicOr(diverged, 1);
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        T* dst = static_cast<T*>(pp.dst[i]);
+        if constexpr (S::kExact)
+            *reinterpret_cast<typename S::T2*>(dst + c) = S::enc2(v[i].x, v[i].y, L::w(i));
+        else
+            *reinterpret_cast<typename S::T2*>(dst + c) = S::pack2(v[i].x, v[i].y);
+    });
 }
 
 template <int Q, class S>
@@ -321,9 +318,16 @@ static cudaError_t bulk_t(const void* fin, void* fout, const uint32_t* bits, con
     if (g.wpr > 2 && g.ny > 2 && zi1 > zi0) {
         const unsigned gy = (unsigned)((g.ny - 2 + kBulkRows - 1) / kBulkRows);
         if (g.nx % 2 == 0) {  // pairs start on even cells
+            PlanePtrs pp{};
+            for (int i = 0; i < Q; ++i) {
+                const long long off = (long long)Lattice<Q>::ex(i) + (long long)Lattice<Q>::ey(i) * g.nx +
+                                      (long long)Lattice<Q>::ez(i) * g.nxy;
+                pp.src[i] = (const typename S::T*)fin + ((long long)i * (long long)g.n - off);
+                pp.dst[i] = (typename S::T*)fout + (size_t)i * g.n;
+            }
             dim3 grid((unsigned)((g.wpr - 2 + 1) / 2), gy, (unsigned)(zi1 - zi0));
             k_bulk_interior2<Q, S><<<grid, block, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout, bits, g, p,
-                                                          zi0, dv);
+                                                          pp, zi0, dv);
         } else {
             dim3 grid((unsigned)(g.wpr - 2), gy, (unsigned)(zi1 - zi0));
             k_bulk_interior<Q, S><<<grid, block, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout, bits, g, p,
