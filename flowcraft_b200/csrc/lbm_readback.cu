@@ -10,7 +10,10 @@
 // 16-byte-per-cell macro buffer the way the reference's GPU kernel does
 // (shaders/lbm_step.comp.glsl:360-363), which saves 16 B of HBM traffic per
 // cell update.
+#include <mutex>
+
 #include "collide.cuh"
+#include "fc_lbm.h"
 #include "lbm_internal.h"
 #include "storage.cuh"
 
@@ -323,3 +326,64 @@ cudaError_t launch_stats(int q, int storage, const void* f, const uint8_t* solid
 }
 
 }  // namespace fc
+
+// ---- statistics without allocation (fc_lbm_stats_noalloc) ----
+// The same k_stats / k_stats_final kernels as fc_lbm_readback_stats, with the
+// per-block partials in a fixed file-scope device array instead of memory the
+// solver allocated: one block per 2^17 cells, at most 4096 blocks, so the
+// array is 4096 * 12 doubles = 384 KiB and covers up to 2^29 cells. Each
+// launch writes every slot of the partials it uses before the final kernel
+// reads them, so nothing has to be cleared between calls.
+namespace {
+
+constexpr int kNoAllocMaxBlocks = 4096;
+constexpr size_t kNoAllocCellsPerBlock = size_t(1) << 17;
+static_assert((unsigned long long)kNoAllocMaxBlocks * kNoAllocCellsPerBlock == FC_LBM_NOALLOC_MAX_CELLS,
+              "header limit must match the scratch size");
+static_assert(fc::kStatsSlots == FC_LBM_STATS_SLOTS, "slot count must match the header");
+
+static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxBlocks * fc::kStatsSlots];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_scratch[kNoAllocMaxDevices] = {};
+
+}  // namespace
+
+extern "C" FC_LBM_API int fc_lbm_stats_noalloc(const void* populations, const uint8_t* solid,
+                                               const float* signed_distance, int32_t nx, int32_t ny, int32_t nz,
+                                               int32_t model, int32_t storage, double* out_slots, void* stream) {
+    if (!populations || !solid || !out_slots) return FC_LBM_ERR_INVALID_ARG;
+    if (nx <= 0 || ny <= 0 || nz <= 0) return FC_LBM_ERR_INVALID_ARG;
+    if (model != FC_LATTICE_D3Q15 && model != FC_LATTICE_D3Q19) return FC_LBM_ERR_INVALID_ARG;
+    if (storage < FC_STORAGE_FP32 || storage > FC_STORAGE_BF16_OFFSET) return FC_LBM_ERR_INVALID_ARG;
+    const size_t n = (size_t)nx * (size_t)ny * (size_t)nz;
+    if (n > FC_LBM_NOALLOC_MAX_CELLS) return FC_LBM_ERR_TOO_LARGE;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return FC_LBM_ERR_CUDA;
+    if (dev >= kNoAllocMaxDevices) return FC_LBM_ERR_UNSUPPORTED;
+    double* scratch = nullptr;
+    {
+        // set-up, once per device, with that device current: the symbol's
+        // host-side name is not a device address
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_scratch[dev]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) return FC_LBM_ERR_CUDA;
+            g_noalloc_scratch[dev] = static_cast<double*>(p);
+        }
+        scratch = g_noalloc_scratch[dev];
+    }
+    fc::Geom g{};
+    g.nx = nx;
+    g.ny = ny;
+    g.nz = nz;
+    g.wpr = (nx + 31) / 32;
+    g.nxy = (long long)nx * ny;
+    g.n = n;
+    const int blocks = (int)((n + kNoAllocCellsPerBlock - 1) / kNoAllocCellsPerBlock);
+    const int q = model == FC_LATTICE_D3Q19 ? 19 : 15;
+    const cudaError_t e = fc::launch_stats(q, storage, populations, solid, signed_distance, g, scratch, blocks,
+                                           out_slots, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? FC_LBM_OK : FC_LBM_ERR_CUDA;
+}

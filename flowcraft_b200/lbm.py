@@ -30,6 +30,7 @@ FC_LBM_ERR_CUDA = -3
 FC_LBM_ERR_TIMEOUT = -4
 FC_LBM_ERR_NOT_INITIALIZED = -5
 FC_LBM_ERR_UNSUPPORTED = -6
+FC_LBM_ERR_TOO_LARGE = -7
 
 FC_MEMORY_HOST = 0
 FC_MEMORY_DEVICE = 1
@@ -122,6 +123,7 @@ SIGNATURES = {
     "fc_lbm_step_timed": (ctypes.c_int, [_P, _I32, _FP, _FP, _FP]),
     "fc_lbm_save_populations": (ctypes.c_int, [_P, _FP, _SZ]),
     "fc_lbm_load_populations": (ctypes.c_int, [_P, _FP, _SZ]),
+    "fc_lbm_stats_noalloc": (ctypes.c_int, [_P, _P, _P, _I32, _I32, _I32, _I32, _I32, _P, _P]),
 }
 
 _lib = None

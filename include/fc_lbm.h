@@ -209,6 +209,39 @@ FC_LBM_API int fc_lbm_save_populations(fc_lbm* h, float* out, size_t count);
 /* Restores a state written by fc_lbm_save_populations (Q*N floats). */
 FC_LBM_API int fc_lbm_load_populations(fc_lbm* h, const float* in, size_t count);
 
+/* Statistics of a population set computed without allocating anything: no
+ * cudaMalloc, cudaFree or allocating library call happens inside. This entry
+ * point has no counterpart in the reference. It is meant for callers that
+ * cannot allocate device memory: applications whose own pool allocator owns
+ * all of the GPU's memory, runs under a fixed memory budget that must not hit
+ * out-of-memory halfway through, and latency-critical loops in which a
+ * cudaMalloc or cudaFree could synchronize the device and stall stepping.
+ *
+ * All pointers are device memory on the calling thread's current device:
+ * `populations` holds Q*N values in `storage`'s format (FC_STORAGE_*), laid
+ * out f[i*N + cell] with N = nx*ny*nz; `solid` holds N bytes;
+ * `signed_distance` holds N floats or is NULL. The result is written to the
+ * device buffer `out_slots` (FC_LBM_STATS_SLOTS doubles: density sum, speed
+ * sum, mass, Fx, Fy, Fz, fluid cell count, min density, max density, max
+ * speed, max stress, NaN flag), asynchronously on `stream` (a cudaStream_t;
+ * NULL = the default stream).
+ *
+ * The reduction's per-block partial sums live in one fixed 384 KiB array
+ * inside the library, which every GPU that loads the library holds until the
+ * process exits. It covers lattices up to FC_LBM_NOALLOC_MAX_CELLS cells;
+ * larger ones are refused with FC_LBM_ERR_TOO_LARGE before any work is
+ * queued. The first call on each device looks up that array's device address
+ * once; make that first call before any stream capture begins. Every call
+ * reuses the same array, so two calls whose work overlaps on the GPU (on
+ * different streams without ordering) race; order them on one stream or with
+ * events. */
+#define FC_LBM_STATS_SLOTS 12
+#define FC_LBM_NOALLOC_MAX_CELLS 536870912ull
+#define FC_LBM_ERR_TOO_LARGE (-7)
+FC_LBM_API int fc_lbm_stats_noalloc(const void* populations, const uint8_t* solid, const float* signed_distance,
+                                    int32_t nx, int32_t ny, int32_t nz, int32_t model, int32_t storage,
+                                    double* out_slots, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
