@@ -54,7 +54,7 @@ __device__ __forceinline__ float2 edotu2(float2 ux, float2 uy, float2 uz) {
 
 // Offset-space collision (collide_offsets) for two cells with FFMA2.
 template <int Q>
-__device__ __forceinline__ bool collide_offsets2(float2 (&h)[Q], float tau, float cs) {
+__device__ __forceinline__ unsigned collide_offsets2(float2 (&h)[Q], float tau, float cs) {
     using L = Lattice<Q>;
     constexpr int NP = (Q - 1) / 2;
     constexpr float si = 1.0f / 256.0f;
@@ -95,8 +95,9 @@ __device__ __forceinline__ bool collide_offsets2(float2 (&h)[Q], float tau, floa
     const float2 isi = mul2(inv, bc2(si));
     const float2 ux = mul2(jx, isi), uy = mul2(jy, isi), uz = mul2(jz, isi);
     const float2 u2 = fma2(ux, ux, fma2(uy, uy, mul2(uz, uz)));
-    const bool bad = !(rho.x > 0.0f && rho.x < __int_as_float(0x7f800000) && u2.x <= 4.0f) ||
-                     !(rho.y > 0.0f && rho.y < __int_as_float(0x7f800000) && u2.y <= 4.0f);
+    // bit 0: cell A trips the divergence test, bit 1: cell B
+    const unsigned bad = (rho.x > 0.0f && rho.x < __int_as_float(0x7f800000) && u2.x <= 4.0f ? 0u : 1u) |
+                         (rho.y > 0.0f && rho.y < __int_as_float(0x7f800000) && u2.y <= 4.0f ? 0u : 2u);
 
     // Pi_neq = 2^-8 S - drho/3 I - rho u u, with the negations folded into
     // constants so every step is one FFMA2 / FMUL2

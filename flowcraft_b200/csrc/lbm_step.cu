@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(32 * kBulkRows) k_bulk_interior2(const typenam
             v[i] = make_float2(a[i], b[i]);
         });
     } else {
-        bad = collide_offsets2<Q>(v, p.tau, p.cs);
+        bad = collide_offsets2<Q>(v, p.tau, p.cs) != 0u;
     }
     if (bad) atomicOr(diverged, 1);
     static_for<0, Q>([&](auto I) {
@@ -204,6 +204,174 @@ __global__ void __launch_bounds__(32 * kBulkRows) k_bulk_interior2(const typenam
             *reinterpret_cast<typename S::T2*>(dst + c) = S::enc2(v[i].x, v[i].y, L::w(i));
         else
             *reinterpret_cast<typename S::T2*>(dst + c) = S::pack2(v[i].x, v[i].y);
+    });
+}
+
+// One inlet or outlet cell (x = 0 or x = nx-1, fluid): equilibrium at the
+// inlet (LbmReference.cpp:269-273); at the outlet, equilibrium from the
+// upstream neighbour's fIn moments with rho relaxed toward 1
+// (LbmReference.cpp:275-327).
+template <int Q, class S>
+__device__ __forceinline__ void plane_cell(const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
+                                           const Geom& g, const StepParams& p, int x, size_t c) {
+    float f[Q];
+    if (x == p.inlet_x) {
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            f[i] = p.feq_inlet[i];
+        });
+    } else {
+        const size_t nb = p.reverse ? c + 1 : c - 1;
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            f[i] = load_pop_c<Q, S, i>(fin, g.n, nb);
+        });
+        float nr, nu, nv, nw;
+        moments<Q>(f, nr, nu, nv, nw);
+        const float rho = nr > 1e-6f ? 1.0f + 0.999f * (nr - 1.0f) : 1.0f;
+        equilibrium_all<Q>(rho, nu, nv, nw, f);
+    }
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        store_pop_c<Q, S, i>(fout, g.n, c, f[i]);
+    });
+}
+
+// Both cells of a pair through the collision the storage format uses;
+// returns a two-bit divergence mask (bit 0: cell A, bit 1: cell B).
+template <int Q, class S>
+__device__ __forceinline__ unsigned collide_pair(float2 (&v)[Q], float tau, float cs) {
+    if constexpr (S::kExact) {  // bit-exact path: the scalar reference-order collision per cell
+        float a[Q], b[Q];
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            a[i] = v[i].x;
+            b[i] = v[i].y;
+        });
+        const unsigned bad = (collide_regularized<Q>(a, tau, cs) ? 1u : 0u) | (collide_regularized<Q>(b, tau, cs) ? 2u : 0u);
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            v[i] = make_float2(a[i], b[i]);
+        });
+        return bad;
+    } else {
+        return collide_offsets2<Q>(v, tau, cs);
+    }
+}
+
+// Bulk cells of lattices with even nx, two x-adjacent cells per thread, every
+// row and every 64-cell chunk. A warp covers cells [64*blockIdx.x, +64) of one
+// row, so whether it touches a Y/Z domain face (`face`) or the first or last
+// chunk of the row (`edge`) is uniform across the warp:
+//   * interior warps run the pure pair pull (aligned 2-element loads for the
+//     e_x = 0 directions, pair stores);
+//   * face and edge warps run the general pair path: sources off the Y/Z edge
+//     come from the cell's own mirrored / bounced plane (the choice is per
+//     direction and uniform across the row), cells that are not bulk cells
+//     here keep in-bounds addresses and are not stored; the lane holding
+//     an x = 0 or x = nx-1 cell also updates that inlet / outlet cell.
+template <int Q, class S>
+__global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs(const typename S::T* __restrict__ fin,
+                                                                typename S::T* __restrict__ fout,
+                                                                const uint32_t* __restrict__ bulk_bits, Geom g,
+                                                                StepParams p, PlanePtrs pp, int z0,
+                                                                int* __restrict__ diverged) {
+    using L = Lattice<Q>;
+    using T = typename S::T;
+    const int y = blockIdx.y * kBulkRows + threadIdx.y;
+    const int z = z0 + blockIdx.z;
+    if (y >= g.ny) return;
+    const size_t row = (size_t)z * g.ny + y;
+    const int k = 2 * threadIdx.x;
+    const int w = 2 * blockIdx.x + (k >> 5);
+    const uint32_t bits = w < g.wpr ? __ldg(bulk_bits + row * g.wpr + w) : 0u;
+    const int x = 64 * blockIdx.x + k;
+    unsigned pair = (bits >> (k & 31)) & 3u;
+    unsigned plane = 0;  // fluid inlet / outlet cells of this pair
+    if (x == 0) {
+        plane |= pair & 1u;
+        pair &= ~1u;
+    }
+    if (x + 1 == g.nx - 1) {
+        plane |= pair & 2u;
+        pair &= ~2u;
+    }
+    if (!(pair | plane)) return;
+    const uint32_t c = (uint32_t)(row * g.nx + x);
+    const bool face = (y == 0) | (y == g.ny - 1) | (z == 0) | (z == g.nz - 1);
+    const bool edge = (blockIdx.x == 0) | (64 * (int)blockIdx.x + 64 >= g.nx);
+
+    float2 v[Q];
+    if (!face && !edge) {
+        if (pair != 3u) {  // one of the two is next to a wall (a boundary-list cell)
+            const uint32_t cc = pair == 1u ? c : c + 1u;
+            bulk_cell<Q, S, false>(fin, fout, g, p, x + (pair == 1u ? 0 : 1), y, z, cc, diverged);
+            return;
+        }
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            const T* src = static_cast<const T*>(pp.src[i]);
+            if constexpr (S::kExact) {
+                v[i] = L::ex(i) == 0 ? S::dec2(S::ld2(src + c), L::w(i))
+                                     : make_float2(S::dec(S::ld(src + c), L::w(i)),
+                                                   S::dec(S::ld(src + c + 1u), L::w(i)));
+            } else {
+                v[i] = L::ex(i) == 0 ? S::raw2(S::ld2(src + c))
+                                     : make_float2(S::raw(S::ld(src + c)), S::raw(S::ld(src + c + 1u)));
+            }
+        });
+        if (collide_pair<Q, S>(v, p.tau, p.cs)) atomicOr(diverged, 1);
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            T* dst = static_cast<T*>(pp.dst[i]);
+            if constexpr (S::kExact)
+                *reinterpret_cast<typename S::T2*>(dst + c) = S::enc2(v[i].x, v[i].y, L::w(i));
+            else
+                *reinterpret_cast<typename S::T2*>(dst + c) = S::pack2(v[i].x, v[i].y);
+        });
+        return;
+    }
+    // general pair path (face rows, first / last chunk of a row); the one
+    // lane of a row end that holds an inlet or outlet cell finishes it alone
+    if (plane) plane_cell<Q, S>(fin, fout, g, p, plane == 1u ? x : x + 1, plane == 1u ? c : (size_t)c + 1);
+    if (!pair) return;
+    const bool va = pair & 1u, vb = pair & 2u;
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        const int py = y - L::ey(i), pz = z - L::ez(i);
+        const bool oy = py < 0 || py >= g.ny;
+        const bool oz = pz < 0 || pz >= g.nz;
+        const bool out = oy || oz;  // the same for the whole row
+        const int plane = out ? edge_plane<Q, i>(oy, oz, p) : i;
+        const uint32_t off = out ? 0u : (uint32_t)link_offset<Q>(i, g);
+        const uint32_t sa = va ? c - off : c;
+        const uint32_t sb = vb ? c + 1u - off : c + 1u;
+        const T* base = fin + (size_t)plane * g.n;
+        if constexpr (S::kExact)
+            v[i] = make_float2(S::dec(S::ld(base + sa), L::w(i)), S::dec(S::ld(base + sb), L::w(i)));
+        else
+            v[i] = make_float2(S::raw(S::ld(base + sa)), S::raw(S::ld(base + sb)));
+    });
+    const unsigned bad = collide_pair<Q, S>(v, p.tau, p.cs) & pair;
+    if (bad) atomicOr(diverged, 1);
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        T* dst = static_cast<T*>(pp.dst[i]);
+        if (pair == 3u) {
+            if constexpr (S::kExact)
+                *reinterpret_cast<typename S::T2*>(dst + c) = S::enc2(v[i].x, v[i].y, L::w(i));
+            else
+                *reinterpret_cast<typename S::T2*>(dst + c) = S::pack2(v[i].x, v[i].y);
+        } else {
+            if constexpr (S::kExact) {
+                if (va) dst[c] = S::enc(v[i].x, L::w(i));
+                if (vb) dst[c + 1u] = S::enc(v[i].y, L::w(i));
+            } else {
+                const typename S::T2 h = S::pack2(v[i].x, v[i].y);
+                if (va) dst[c] = h.x;
+                if (vb) dst[c + 1u] = h.y;
+            }
+        }
     });
 }
 
@@ -313,26 +481,27 @@ static cudaError_t bulk_t(const void* fin, void* fout, const uint32_t* bits, con
     if (zc <= 0) return cudaSuccess;
     const int z1 = z0 + zc;
     dim3 block(32, kBulkRows, 1);
-    // interior: chunks 1..wpr-2, rows 1..ny-2, z in [max(z0,1), min(z1,nz-1))
+    if (g.nx % 2 == 0) {  // pairs start on even cells: every row through k_bulk_pairs
+        PlanePtrs pp{};
+        for (int i = 0; i < Q; ++i) {
+            const long long off = (long long)Lattice<Q>::ex(i) + (long long)Lattice<Q>::ey(i) * g.nx +
+                                  (long long)Lattice<Q>::ez(i) * g.nxy;
+            pp.src[i] = (const typename S::T*)fin + ((long long)i * (long long)g.n - off);
+            pp.dst[i] = (typename S::T*)fout + (size_t)i * g.n;
+        }
+        dim3 grid((unsigned)((g.nx + 63) / 64), (unsigned)((g.ny + kBulkRows - 1) / kBulkRows), (unsigned)zc);
+        k_bulk_pairs<Q, S><<<grid, block, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout, bits, g, p, pp, z0,
+                                                  dv);
+        ++*launched;
+        return cudaGetLastError();
+    }
+    // odd nx: one-cell interior kernel + shell kernel (planes ride in the shell's row-end warps)
     const int zi0 = z0 > 1 ? z0 : 1, zi1 = z1 < g.nz - 1 ? z1 : g.nz - 1;
     if (g.wpr > 2 && g.ny > 2 && zi1 > zi0) {
         const unsigned gy = (unsigned)((g.ny - 2 + kBulkRows - 1) / kBulkRows);
-        if (g.nx % 2 == 0) {  // pairs start on even cells
-            PlanePtrs pp{};
-            for (int i = 0; i < Q; ++i) {
-                const long long off = (long long)Lattice<Q>::ex(i) + (long long)Lattice<Q>::ey(i) * g.nx +
-                                      (long long)Lattice<Q>::ez(i) * g.nxy;
-                pp.src[i] = (const typename S::T*)fin + ((long long)i * (long long)g.n - off);
-                pp.dst[i] = (typename S::T*)fout + (size_t)i * g.n;
-            }
-            dim3 grid((unsigned)((g.wpr - 2 + 1) / 2), gy, (unsigned)(zi1 - zi0));
-            k_bulk_interior2<Q, S><<<grid, block, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout, bits, g, p,
-                                                          pp, zi0, dv);
-        } else {
-            dim3 grid((unsigned)(g.wpr - 2), gy, (unsigned)(zi1 - zi0));
-            k_bulk_interior<Q, S><<<grid, block, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout, bits, g, p,
-                                                         zi0, dv);
-        }
+        dim3 grid((unsigned)(g.wpr - 2), gy, (unsigned)(zi1 - zi0));
+        k_bulk_interior<Q, S><<<grid, block, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout, bits, g, p, zi0,
+                                                     dv);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         ++*launched;
