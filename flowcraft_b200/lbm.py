@@ -87,6 +87,10 @@ class _Stats(ctypes.Structure):
     ]
 
 
+class _VoxelParams(ctypes.Structure):
+    _fields_ = [("target_resolution", ctypes.c_int32), ("padding", ctypes.c_float * 3)]
+
+
 # Every function the header declares, with its ctypes signature.
 _P = ctypes.c_void_p
 _I32 = ctypes.c_int32
@@ -124,6 +128,8 @@ SIGNATURES = {
     "fc_lbm_save_populations": (ctypes.c_int, [_P, _FP, _SZ]),
     "fc_lbm_load_populations": (ctypes.c_int, [_P, _FP, _SZ]),
     "fc_lbm_stats_noalloc": (ctypes.c_int, [_P, _P, _P, _I32, _I32, _I32, _I32, _I32, _P, _P]),
+    "fc_lbm_voxel_grid": (ctypes.c_int, [_P, _SZ, ctypes.POINTER(_VoxelParams), _I32, _I32P, _FP, _FP, _P]),
+    "fc_lbm_voxelize": (ctypes.c_int, [_P, _SZ, _P, _SZ, _I32P, ctypes.c_float, _FP, _I32, _P, _P, _P]),
 }
 
 _lib = None

@@ -242,6 +242,43 @@ FC_LBM_API int fc_lbm_stats_noalloc(const void* populations, const uint8_t* soli
                                     int32_t nx, int32_t ny, int32_t nz, int32_t model, int32_t storage,
                                     double* out_slots, void* stream);
 
+/* ---- Mesh voxelizer ----
+ * Replaces Voxelizer::Voxelize (FlowCraft/Voxelizer.h:44-45,
+ * Voxelizer.cpp:136-485), the producer of the VoxelGrid that fc_lbm_init
+ * consumes. The results are bit-identical to the reference's CPU voxelizer:
+ * the same cells, the same solid mask and the same float signed distances
+ * (positive in the fluid, negative in the solid, +-infinity where no triangle
+ * came within reach), computed on the current device. Positions are float
+ * triples (x, y, z) in world units; indices are uint32 triples, one per
+ * triangle, any trailing remainder ignored as in the reference. Grid x spans
+ * world y (the flow axis) and grid y spans world x (VoxelGrid.h:43-56). With
+ * `memory` = FC_MEMORY_DEVICE every array is device memory on the current
+ * device; with FC_MEMORY_HOST every array is host memory. Both calls block
+ * until their results are ready; their work runs on `stream` (a cudaStream_t;
+ * NULL = the default stream). */
+typedef struct fc_voxel_params {
+    int32_t target_resolution; /* cells along the padded domain's longest axis; reference default 640 */
+    float padding[3];          /* padding per side as a fraction of the model's extent; default {0.3, 1.0, 0.5} */
+} fc_voxel_params;
+
+/* The grid Voxelize derives for a mesh (Voxelizer.cpp:146-166): dims (nx, ny,
+ * nz), cell size and world origin of the padded domain. The caller handles the
+ * reference's empty-grid case (no vertices or fewer than 3 indices) itself;
+ * vertex_count = 0 returns FC_LBM_ERR_INVALID_ARG. */
+FC_LBM_API int fc_lbm_voxel_grid(const float* positions, size_t vertex_count, const fc_voxel_params* params,
+                                 int32_t memory, int32_t dims[3], float* cell_size, float origin[3], void* stream);
+
+/* Voxelizes the mesh onto an explicit grid: `solid` receives nx*ny*nz bytes
+ * (0 fluid, 1 solid) and `signed_distance` nx*ny*nz floats, indexed
+ * (z*ny + y)*nx + x. On the grid from fc_lbm_voxel_grid this is
+ * Voxelizer::Voxelize; any other grid (a chosen cell size and origin) runs the
+ * same rasterization, flood fill from cell (0,0,0) and sign reconciliation.
+ * Returns FC_LBM_ERR_INVALID_ARG for an index outside the vertex array, and
+ * FC_LBM_ERR_TOO_LARGE for grids of 2^32-1 cells or more. */
+FC_LBM_API int fc_lbm_voxelize(const float* positions, size_t vertex_count, const uint32_t* indices,
+                               size_t index_count, const int32_t dims[3], float cell_size, const float origin[3],
+                               int32_t memory, uint8_t* solid, float* signed_distance, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

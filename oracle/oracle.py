@@ -206,3 +206,83 @@ class Oracle:
         s = OracleStats()
         self.api["stats"](self.h, ctypes.byref(s))
         return s.as_dict()
+
+
+# ---- voxelizer oracle (voxel_oracle.c) and the reference's Voxelizer ----
+def _vox_lib(kind: str):
+    key = "vox_" + kind
+    if key in _loaded:
+        return _loaded[key]
+    if kind == "oracle":
+        path = os.path.join(HERE, "libvoxel_oracle.so")
+        if not os.path.exists(path):
+            build()
+        lib = ctypes.CDLL(path)
+        lib.voxo_grid_for_mesh.restype = ctypes.c_int
+        lib.voxo_grid_for_mesh.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_float,
+                                           ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p]
+        lib.voxo_voxelize.restype = ctypes.c_int
+        lib.voxo_voxelize.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
+                                      ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p]
+    else:
+        lib = ctypes.CDLL(_LIBS["ref"][0])
+        lib.ref_voxelize.restype = ctypes.c_void_p
+        lib.ref_voxelize.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
+                                     ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float]
+        lib.ref_voxels_info.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        lib.ref_voxels_copy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        lib.ref_voxels_free.argtypes = [ctypes.c_void_p]
+    _loaded[key] = lib
+    return lib
+
+
+def grid_for_mesh(positions, target_resolution=640, padding=(0.3, 1.0, 0.5)):
+    """Voxelizer::Voxelize's grid for a mesh: ((nx, ny, nz), cell_size, origin)."""
+    lib = _vox_lib("oracle")
+    pos = np.ascontiguousarray(positions, dtype=np.float32)
+    dims = np.zeros(3, dtype=np.int32)
+    cell = np.zeros(1, dtype=np.float32)
+    origin = np.zeros(3, dtype=np.float32)
+    rc = lib.voxo_grid_for_mesh(pos.ctypes.data, len(pos), int(target_resolution), *[float(p) for p in padding],
+                                dims.ctypes.data, cell.ctypes.data, origin.ctypes.data)
+    if rc != 0:
+        raise ValueError("empty mesh")
+    return tuple(int(d) for d in dims), float(cell[0]), origin
+
+
+def voxelize(positions, indices, dims, cell_size, origin, impl: str = "oracle"):
+    """(solid u8 (nz,ny,nx), sdf f32 (nz,ny,nx)) on the given grid."""
+    pos = np.ascontiguousarray(positions, dtype=np.float32)
+    idx = np.ascontiguousarray(indices, dtype=np.uint32)
+    nx, ny, nz = dims
+    solid = np.empty(nx * ny * nz, dtype=np.uint8)
+    sdf = np.empty(nx * ny * nz, dtype=np.float32)
+    d = np.asarray(dims, dtype=np.int32)
+    o = np.ascontiguousarray(origin, dtype=np.float32)
+    lib = _vox_lib("oracle")
+    rc = lib.voxo_voxelize(pos.ctypes.data, len(pos), idx.ctypes.data, idx.size, d.ctypes.data, float(cell_size),
+                           o.ctypes.data, solid.ctypes.data, sdf.ctypes.data)
+    if rc != 0:
+        raise MemoryError("voxelizer oracle failed")
+    return solid.reshape(nz, ny, nx), sdf.reshape(nz, ny, nx)
+
+
+def voxelize_reference(positions, indices, target_resolution=640, padding=(0.3, 1.0, 0.5)):
+    """FlowCraft's own Voxelizer::Voxelize (oracle/_ref): (dims, cell, origin, solid, sdf)."""
+    lib = _vox_lib("ref")
+    pos = np.ascontiguousarray(positions, dtype=np.float32)
+    idx = np.ascontiguousarray(indices, dtype=np.uint32)
+    h = lib.ref_voxelize(pos.ctypes.data, len(pos), idx.ctypes.data, idx.size, int(target_resolution),
+                         *[float(p) for p in padding])
+    dims = np.zeros(3, dtype=np.int32)
+    cell = np.zeros(1, dtype=np.float32)
+    origin = np.zeros(3, dtype=np.float32)
+    lib.ref_voxels_info(h, dims.ctypes.data, cell.ctypes.data, origin.ctypes.data)
+    nx, ny, nz = (int(v) for v in dims)
+    solid = np.empty(nx * ny * nz, dtype=np.uint8)
+    sdf = np.empty(nx * ny * nz, dtype=np.float32)
+    lib.ref_voxels_copy(h, solid.ctypes.data, sdf.ctypes.data)
+    lib.ref_voxels_free(h)
+    return (nx, ny, nz), float(cell[0]), origin, solid.reshape(nz, ny, nx), sdf.reshape(nz, ny, nx)

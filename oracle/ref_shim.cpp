@@ -104,3 +104,44 @@ void ref_stats(ref_lbm* r, oracle_stats* s) {
 }
 
 }  // extern "C"
+
+// ---- Voxelizer (FlowCraft/Voxelizer.cpp:136-485) ----
+#include "Voxelizer.h"
+
+extern "C" {
+
+struct ref_voxels {
+    VoxelGrid grid;
+};
+
+ref_voxels* ref_voxelize(const float* positions, size_t vertex_count, const uint32_t* indices, size_t index_count,
+                         int target_resolution, float pad_x, float pad_y, float pad_z) {
+    std::vector<Vec3> pos(vertex_count);
+    for (size_t i = 0; i < vertex_count; ++i) pos[i] = Vec3(positions[3 * i], positions[3 * i + 1], positions[3 * i + 2]);
+    std::vector<uint32_t> idx(indices, indices + index_count);
+    Voxelizer::Params p;
+    p.targetResolution = target_resolution;
+    p.paddingFactor = Vec3(pad_x, pad_y, pad_z);
+    ref_voxels* v = new ref_voxels();
+    v->grid = Voxelizer::Voxelize(pos, idx, p);
+    return v;
+}
+
+void ref_voxels_info(const ref_voxels* v, int* dims, float* cell_size, float* origin) {
+    dims[0] = v->grid.nx;
+    dims[1] = v->grid.ny;
+    dims[2] = v->grid.nz;
+    *cell_size = v->grid.cellSize;
+    origin[0] = v->grid.origin.x;
+    origin[1] = v->grid.origin.y;
+    origin[2] = v->grid.origin.z;
+}
+
+void ref_voxels_copy(const ref_voxels* v, uint8_t* solid, float* sdf) {
+    std::memcpy(solid, v->grid.solid.data(), v->grid.solid.size());
+    std::memcpy(sdf, v->grid.signedDistance.data(), v->grid.signedDistance.size() * sizeof(float));
+}
+
+void ref_voxels_free(ref_voxels* v) { delete v; }
+
+}  // extern "C"
