@@ -166,4 +166,55 @@ private:
     int32_t nx_ = 0, ny_ = 0, nz_ = 0;
 };
 
+// Voxelizer::Voxelize (FlowCraft/Voxelizer.h:12-53) on the GPU, bit-identical
+// to the reference's CPU voxelizer. `Grid` is any type with the fields of
+// FlowCraft's VoxelGrid (nx, ny, nz, cellSize, origin.{x,y,z}, solid,
+// signedDistance), `Vec` any type with float members x, y, z. Runs on the
+// current CUDA device and blocks until the grid is on the host. Returns false
+// (grid left empty) when the CUDA call fails, with the status in *status.
+struct VoxelizerParams {
+    int targetResolution = 640;
+    Vec3f paddingFactor{0.3f, 1.0f, 0.5f};
+};
+
+template <class Grid, class Vec>
+bool Voxelize(const std::vector<Vec>& positions, const std::vector<uint32_t>& indices, const VoxelizerParams& params,
+              Grid& grid, int* status = nullptr) {
+    grid = Grid{};
+    if (status) *status = FC_LBM_OK;
+    if (positions.empty() || indices.size() < 3) return true;  // the reference's empty grid
+    std::vector<float> pos(positions.size() * 3);
+    for (size_t i = 0; i < positions.size(); ++i) {
+        pos[3 * i] = positions[i].x;
+        pos[3 * i + 1] = positions[i].y;
+        pos[3 * i + 2] = positions[i].z;
+    }
+    fc_voxel_params p{params.targetResolution,
+                      {params.paddingFactor.x, params.paddingFactor.y, params.paddingFactor.z}};
+    int32_t dims[3] = {0, 0, 0};
+    float cell = 0.0f, origin[3] = {0.0f, 0.0f, 0.0f};
+    int rc = fc_lbm_voxel_grid(pos.data(), positions.size(), &p, FC_MEMORY_HOST, dims, &cell, origin, nullptr);
+    std::vector<uint8_t> solid;
+    std::vector<float> sdf;
+    if (rc == FC_LBM_OK) {
+        const size_t n = (size_t)dims[0] * dims[1] * dims[2];
+        solid.resize(n);
+        sdf.resize(n);
+        rc = fc_lbm_voxelize(pos.data(), positions.size(), indices.data(), indices.size(), dims, cell, origin,
+                             FC_MEMORY_HOST, solid.data(), sdf.data(), nullptr);
+    }
+    if (status) *status = rc;
+    if (rc != FC_LBM_OK) return false;
+    grid.nx = dims[0];
+    grid.ny = dims[1];
+    grid.nz = dims[2];
+    grid.cellSize = cell;
+    grid.origin.x = origin[0];
+    grid.origin.y = origin[1];
+    grid.origin.z = origin[2];
+    grid.solid = std::move(solid);
+    grid.signedDistance = std::move(sdf);
+    return true;
+}
+
 }  // namespace fc

@@ -1,5 +1,6 @@
 """The C++ host mirror (include/fc_lbm_solver.hpp) compiles against the C ABI
-and links; on a GPU, the restated reference test passes bit-for-bit."""
+and links; on a GPU, the restated reference test passes bit-for-bit and
+fc::Voxelize matches the voxelizer oracle."""
 import os
 import subprocess
 
@@ -15,7 +16,7 @@ def _build(tmp_path):
     lib_dir = os.path.join(ROOT, "flowcraft_b200")
     ora_dir = os.path.join(ROOT, "oracle")
     cmd = ["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-I" + os.path.join(ROOT, "include"), SRC, "-o", exe,
-           "-L" + lib_dir, "-lfc_lbm", "-L" + ora_dir, "-l:liblbm_oracle32.so",
+           "-L" + lib_dir, "-lfc_lbm", "-L" + ora_dir, "-l:liblbm_oracle32.so", "-l:libvoxel_oracle.so",
            "-Wl,-rpath," + lib_dir + ":" + ora_dir, "-pthread"]
     subprocess.run(cmd, check=True, capture_output=True, text=True)
     return exe
@@ -31,4 +32,4 @@ def test_cpp_gpu_vs_cpu(gpu, oracle_built, tmp_path):
     res = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     print(res.stdout)
     assert res.returncode == 0, res.stdout + res.stderr
-    assert res.stdout.count("PASS") == 2
+    assert res.stdout.count("PASS") == 3
