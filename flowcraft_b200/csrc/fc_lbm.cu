@@ -49,6 +49,10 @@ struct fc_lbm {
     double* d_stats_partials = nullptr;
     double* d_stats_result = nullptr;
     int stats_blocks = 0;
+    double* d_aero_partials = nullptr;
+    double* d_aero_result = nullptr;
+    float cell_size = 1.0f;
+    float origin[3] = {0.0f, 0.0f, 0.0f};
     float* d_stage = nullptr;
     float* h_stage = nullptr;
     size_t stage_floats = 0;
@@ -176,6 +180,8 @@ void release(fc_lbm* h) {
     dfree(h->d_diverged);
     dfree(h->d_stats_partials);
     dfree(h->d_stats_result);
+    dfree(h->d_aero_partials);
+    dfree(h->d_aero_result);
     dfree(h->d_stage);
     if (h->h_stage) cudaFreeHost(h->h_stage);
     h->h_stage = nullptr;
@@ -418,6 +424,8 @@ int fc_lbm_init(fc_lbm* h, const fc_grid_desc* grid, int32_t model, const fc_opt
     h->g.ny = grid->ny;
     h->g.nz = grid->nz;
     h->g.wpr = (grid->nx + 31) / 32;
+    h->cell_size = grid->cell_size;
+    for (int k = 0; k < 3; ++k) h->origin[k] = grid->origin[k];
     h->g.nxy = (long long)grid->nx * grid->ny;
     h->g.n = n;
 
@@ -453,6 +461,9 @@ int fc_lbm_init(fc_lbm* h, const fc_grid_desc* grid, int32_t model, const fc_opt
         FC_TRY(h, cudaMalloc(&h->d_stats_partials, (size_t)h->stats_blocks * fc::kStatsSlots * sizeof(double)),
                "alloc stats partials");
         FC_TRY(h, cudaMalloc(&h->d_stats_result, fc::kStatsSlots * sizeof(double)), "alloc stats result");
+        FC_TRY(h, cudaMalloc(&h->d_aero_partials, (size_t)h->stats_blocks * fc::kAeroSlots * sizeof(double)),
+               "alloc force partials");
+        FC_TRY(h, cudaMalloc(&h->d_aero_result, fc::kAeroResult * sizeof(double)), "alloc force result");
         FC_TRY(h, cudaMemsetAsync(h->d_diverged, 0, sizeof(int), h->stream), "clear flag");
         const bool dev = grid->memory == FC_MEMORY_DEVICE;
         FC_RC(upload(h, h->d_solid, grid->solid, n, dev));
@@ -623,6 +634,37 @@ int fc_lbm_readback_stats(fc_lbm* h, fc_stats* out) {
     out->force_z = (float)r[5];
     out->has_nan = r[11] != 0.0;
     out->valid = 1;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_aero_forces(fc_lbm* h, fc_aero_forces* out) {
+    FC_RC(check_ready(h));
+    if (!out) return FC_LBM_ERR_INVALID_ARG;
+    DeviceGuard dg(h->device);
+    FC_TRY(h, fc::launch_aero(h->q, h->storage, h->pop[h->cur], h->d_solid, h->d_sdf, h->g, h->cell_size,
+                              h->origin[0], h->origin[1], h->origin[2], h->d_aero_partials, h->stats_blocks,
+                              h->d_aero_result, h->stream),
+           "force kernel");
+    h->launches += 2;
+    FC_TRY(h, cudaMemcpyAsync(h->h_stage, h->d_aero_result, fc::kAeroResult * sizeof(double), cudaMemcpyDeviceToHost,
+                              h->stream),
+           "force download");
+    FC_RC(wait_stream(h, kTransferTimeoutMs));
+    double r[fc::kAeroResult];
+    std::memcpy(r, h->h_stage, sizeof(r));
+    std::memset(out, 0, sizeof(*out));
+    for (int k = 0; k < 3; ++k) {
+        out->force_sum[k] = r[k];
+        out->force[k] = (float)r[k];
+        out->center_of_pressure[k] = (float)r[9 + k];
+        out->lift_arrow_base[k] = (float)r[12 + k];
+    }
+    out->lift_weight_sum = r[3];
+    out->force_weight_sum = r[4];
+    out->solid_cells = (uint64_t)r[5];
+    out->min_stress = (float)r[6];
+    out->max_stress = (float)r[7];
+    out->has_nan = r[8] != 0.0;
     return FC_LBM_OK;
 }
 

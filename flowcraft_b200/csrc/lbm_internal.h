@@ -103,6 +103,17 @@ int stats_blocks(const Geom& g);
 cudaError_t launch_stats(int q, int storage, const void* f, const uint8_t* solid, const float* sdf, const Geom& g,
                          double* partials, int blocks, double* result, cudaStream_t s);
 
+// Aerodynamic force integral (FieldOverlay::ComputeAerodynamicForces). The
+// partials take stats_blocks(g) * kAeroSlots doubles; `result` receives
+// kAeroResult doubles: force sums (3), lift and force weight sums, solid
+// count, stress range (2), NaN flag, centre of pressure (3), lift arrow base
+// (3).
+constexpr int kAeroSlots = 20;
+constexpr int kAeroResult = 16;
+cudaError_t launch_aero(int q, int storage, const void* f, const uint8_t* solid, const float* sdf, const Geom& g,
+                        float cell_size, float ox, float oy, float oz, double* partials, int blocks, double* result,
+                        cudaStream_t s);
+
 // Setup (geometry classification and boundary-list construction).
 // counts[0] += flagged (boundary-list) cells, counts[1] += bulk cells.
 cudaError_t launch_classify(int q, const uint8_t* solid, const Geom& g, uint8_t* flags, uint32_t* bulk_bits,

@@ -250,6 +250,170 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats_final(const double* __r
     stat_block_reduce(acc, result);
 }
 
+// ---- aerodynamic forces (FieldOverlay::ComputeAerodynamicForces, FieldOverlay.cpp:469-621) ----
+// Slots: 0-2 force sums, 3 lift weight sum, 4-6 lift-weighted position sums,
+// 7 force weight sum, 8-10 force-weighted sums, 11-13 geometric position sums,
+// 14 solid count, 15 max solid z, 16 min loaded stress, 17 max loaded stress,
+// 18 NaN flag. All sums are FP64; a solid cell whose field entry is not finite
+// only raises the flag (the reference skips it after counting its position).
+enum AeroSlot { kAfx = 0, kAlw = 3, kAlwx = 4, kAfw = 7, kAfwx = 8, kAgx = 11, kAcount = 14, kAmaxz = 15,
+                kAlo = 16, kAhi = 17, kAnan = 18 };
+
+__device__ __forceinline__ void aero_init(double* a) {
+    for (int k = 0; k < kAeroSlots; ++k) a[k] = 0.0;
+    a[kAmaxz] = -1.0;
+    a[kAlo] = 1e30;
+    a[kAhi] = -1e30;
+}
+
+__device__ __forceinline__ void aero_merge(double* a, const double* b) {
+    for (int k = 0; k <= kAcount; ++k) a[k] += b[k];
+    a[kAmaxz] = fmax(a[kAmaxz], b[kAmaxz]);
+    a[kAlo] = fmin(a[kAlo], b[kAlo]);
+    a[kAhi] = fmax(a[kAhi], b[kAhi]);
+    a[kAnan] = fmax(a[kAnan], b[kAnan]);
+}
+
+// Block reduction in a fixed order (shuffle tree, then warps in order).
+__device__ void aero_block_reduce(double* a, double* out) {
+    __shared__ double sh[kStatsThreads / 32][kAeroSlots];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        double b[kAeroSlots];
+        for (int k = 0; k < kAeroSlots; ++k) b[k] = __shfl_down_sync(0xffffffffu, a[k], o);
+        aero_merge(a, b);
+    }
+    if (lane == 0)
+        for (int k = 0; k < kAeroSlots; ++k) sh[warp][k] = a[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kStatsThreads / 32; ++w) aero_merge(a, sh[w]);
+        for (int k = 0; k < kAeroSlots; ++k) out[k] = a[k];
+    }
+}
+
+template <int Q, class S>
+__global__ void __launch_bounds__(kStatsThreads) k_aero(const typename S::T* __restrict__ f,
+                                                        const uint8_t* __restrict__ solid,
+                                                        const float* __restrict__ sdf, Geom g, float cs, float ox,
+                                                        float oy, float oz, double* __restrict__ partials) {
+    double a[kAeroSlots];
+    aero_init(a);
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < g.n; c += (size_t)gridDim.x * blockDim.x) {
+        if (!solid[c]) continue;
+        const int z = (int)(c / (size_t)g.nxy);
+        const size_t rem = c - (size_t)z * g.nxy;
+        const int y = (int)(rem / g.nx);
+        const int x = (int)(rem - (size_t)y * g.nx);
+        // VoxelGrid::CellCenter (VoxelGrid.h:53-55) in float
+        const float px = ox + ((float)y + 0.5f) * cs;
+        const float py = oy + ((float)x + 0.5f) * cs;
+        const float pz = oz + ((float)z + 0.5f) * cs;
+        a[kAgx] += (double)px;
+        a[kAgx + 1] += (double)py;
+        a[kAgx + 2] += (double)pz;
+        a[kAcount] += 1.0;
+        a[kAmaxz] = fmax(a[kAmaxz], (double)z);
+        const float4 v = solid_force<Q, S>(f, solid, sdf, g, x, y, z, c);
+        if (!isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z) || !isfinite(v.w)) {
+            a[kAnan] = 1.0;
+            continue;
+        }
+        a[kAfx] += (double)v.y;
+        a[kAfx + 1] += (double)v.z;
+        a[kAfx + 2] += (double)v.w;
+        const double wl = fabs((double)v.w);
+        a[kAlw] += wl;
+        a[kAlwx] += wl * px;
+        a[kAlwx + 1] += wl * py;
+        a[kAlwx + 2] += wl * pz;
+        const double wf = sqrt((double)v.y * v.y + (double)v.z * v.z + (double)v.w * v.w);
+        a[kAfw] += wf;
+        a[kAfwx] += wf * px;
+        a[kAfwx + 1] += wf * py;
+        a[kAfwx + 2] += wf * pz;
+        if (v.x > 0.0f) {
+            a[kAlo] = fmin(a[kAlo], (double)v.x);
+            a[kAhi] = fmax(a[kAhi], (double)v.x);
+        }
+    }
+    aero_block_reduce(a, partials + (size_t)blockIdx.x * kAeroSlots);
+}
+
+// Reduces the partials, then computes the centre of pressure and the lift
+// arrow's base from a 5x5 patch of columns around it (FieldOverlay.cpp:
+// 580-618), one column per thread.
+__global__ void __launch_bounds__(kStatsThreads) k_aero_final(const double* __restrict__ partials, int blocks,
+                                                              const uint8_t* __restrict__ solid, Geom g, float cs,
+                                                              float ox, float oy, float oz,
+                                                              double* __restrict__ result) {
+    __shared__ double tot[kAeroSlots];
+    __shared__ float cp[3];
+    __shared__ int col_top;
+    double a[kAeroSlots];
+    aero_init(a);
+    for (int b = threadIdx.x; b < blocks; b += blockDim.x) aero_merge(a, partials + (size_t)b * kAeroSlots);
+    aero_block_reduce(a, tot);
+    if (threadIdx.x == 0) {
+        col_top = -1;
+        const double lw = tot[kAlw], fw = tot[kAfw], count = tot[kAcount];
+        float c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
+        if (lw > 1e-9) {
+            c0 = (float)(tot[kAlwx] / lw), c1 = (float)(tot[kAlwx + 1] / lw), c2 = (float)(tot[kAlwx + 2] / lw);
+        } else if (fw > 1e-9) {
+            c0 = (float)(tot[kAfwx] / fw), c1 = (float)(tot[kAfwx + 1] / fw), c2 = (float)(tot[kAfwx + 2] / fw);
+        } else if (count > 0.0) {
+            const double inv = 1.0 / count;
+            c0 = (float)(tot[kAgx] * inv), c1 = (float)(tot[kAgx + 1] * inv), c2 = (float)(tot[kAgx + 2] * inv);
+        }
+        cp[0] = c0, cp[1] = c1, cp[2] = c2;
+    }
+    __syncthreads();
+    if (threadIdx.x < 25) {
+        const int nxm = g.nx - 1 > 0 ? g.nx - 1 : 0, nym = g.ny - 1 > 0 ? g.ny - 1 : 0;
+        int gx = (int)floorf((cp[1] - oy) / cs), gy = (int)floorf((cp[0] - ox) / cs);
+        gx = gx < 0 ? 0 : (gx > nxm ? nxm : gx);
+        gy = gy < 0 ? 0 : (gy > nym ? nym : gy);
+        int x = gx + (int)(threadIdx.x % 5) - 2, y = gy + (int)(threadIdx.x / 5) - 2;
+        x = x < 0 ? 0 : (x > nxm ? nxm : x);
+        y = y < 0 ? 0 : (y > nym ? nym : y);
+        for (int z = g.nz - 1; z >= 0; --z)
+            if (solid[((size_t)z * g.ny + y) * g.nx + x]) {
+                atomicMax(&col_top, z);
+                break;
+            }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int maxz = (int)tot[kAmaxz];
+        const int eff = col_top >= 0 ? col_top : (maxz > 0 ? maxz : 0);
+        float lo = (float)tot[kAlo], hi = (float)tot[kAhi];
+        if (lo > hi) {
+            lo = 0.0f;
+            hi = 1e-6f;
+        } else {
+            lo = 0.0f;
+            if (!(hi > lo)) hi = lo + 1e-6f;
+        }
+        result[0] = tot[kAfx];
+        result[1] = tot[kAfx + 1];
+        result[2] = tot[kAfx + 2];
+        result[3] = tot[kAlw];
+        result[4] = tot[kAfw];
+        result[5] = tot[kAcount];
+        result[6] = lo;
+        result[7] = hi;
+        result[8] = tot[kAnan];
+        result[9] = cp[0];
+        result[10] = cp[1];
+        result[11] = cp[2];
+        result[12] = cp[0];
+        result[13] = cp[1];
+        result[14] = oz + ((float)eff + 1.0f) * cs;
+        result[15] = (double)maxz;
+    }
+}
+
 int stats_blocks(const Geom& g) {
     const size_t want = (g.n + kStatsThreads * 8 - 1) / (kStatsThreads * 8);
     const size_t cap = 148 * 16;
@@ -323,6 +487,22 @@ cudaError_t launch_pops_in(int q, int storage, void* f, const Geom& g, size_t ce
 cudaError_t launch_stats(int q, int storage, const void* f, const uint8_t* solid, const float* sdf, const Geom& g,
                          double* partials, int blocks, double* result, cudaStream_t s) {
     FC_DISPATCH(q, storage, stats_t, f, solid, sdf, g, partials, blocks, result, s);
+}
+
+template <int Q, class S>
+static cudaError_t aero_t(const void* f, const uint8_t* solid, const float* sdf, const Geom& g, float cs, float ox,
+                          float oy, float oz, double* partials, int blocks, double* result, cudaStream_t s) {
+    k_aero<Q, S><<<blocks, kStatsThreads, 0, s>>>((const typename S::T*)f, solid, sdf, g, cs, ox, oy, oz, partials);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_aero_final<<<1, kStatsThreads, 0, s>>>(partials, blocks, solid, g, cs, ox, oy, oz, result);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_aero(int q, int storage, const void* f, const uint8_t* solid, const float* sdf, const Geom& g,
+                        float cell_size, float ox, float oy, float oz, double* partials, int blocks, double* result,
+                        cudaStream_t s) {
+    FC_DISPATCH(q, storage, aero_t, f, solid, sdf, g, cell_size, ox, oy, oz, partials, blocks, result, s);
 }
 
 }  // namespace fc

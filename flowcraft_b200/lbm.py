@@ -87,6 +87,14 @@ class _Stats(ctypes.Structure):
     ]
 
 
+class _AeroForces(ctypes.Structure):
+    _fields_ = [("force", ctypes.c_float * 3), ("min_stress", ctypes.c_float), ("max_stress", ctypes.c_float),
+                ("center_of_pressure", ctypes.c_float * 3), ("lift_arrow_base", ctypes.c_float * 3),
+                ("has_nan", ctypes.c_int32), ("force_sum", ctypes.c_double * 3),
+                ("lift_weight_sum", ctypes.c_double), ("force_weight_sum", ctypes.c_double),
+                ("solid_cells", ctypes.c_uint64)]
+
+
 class _VoxelParams(ctypes.Structure):
     _fields_ = [("target_resolution", ctypes.c_int32), ("padding", ctypes.c_float * 3)]
 
@@ -128,6 +136,7 @@ SIGNATURES = {
     "fc_lbm_save_populations": (ctypes.c_int, [_P, _FP, _SZ]),
     "fc_lbm_load_populations": (ctypes.c_int, [_P, _FP, _SZ]),
     "fc_lbm_stats_noalloc": (ctypes.c_int, [_P, _P, _P, _I32, _I32, _I32, _I32, _I32, _P, _P]),
+    "fc_lbm_aero_forces": (ctypes.c_int, [_P, ctypes.POINTER(_AeroForces)]),
     "fc_lbm_voxel_grid": (ctypes.c_int, [_P, _SZ, ctypes.POINTER(_VoxelParams), _I32, _I32P, _FP, _FP, _P]),
     "fc_lbm_voxelize": (ctypes.c_int, [_P, _SZ, _P, _SZ, _I32P, ctypes.c_float, _FP, _I32, _P, _P, _P]),
 }
@@ -209,6 +218,24 @@ class Stats:
     forceSum: tuple = (0.0, 0.0, 0.0)
     fluidCells: int = 0
     extra: dict = field(default_factory=dict)
+
+
+@dataclass
+class AerodynamicForces:
+    """FieldOverlay::AerodynamicForces (FieldOverlay.h:186-195) plus the FP64
+    sums the device integral produces."""
+    forceX: float = 0.0
+    forceY: float = 0.0
+    forceZ: float = 0.0
+    minStress: float = 0.0
+    maxStress: float = 0.0
+    centerOfPressure: tuple = (0.0, 0.0, 0.0)
+    liftArrowBase: tuple = (0.0, 0.0, 0.0)
+    hasNaN: bool = False
+    forceSum: tuple = (0.0, 0.0, 0.0)
+    liftWeightSum: float = 0.0
+    forceWeightSum: float = 0.0
+    solidCells: int = 0
 
 
 def _stream_ptr(cmd) -> int | None:
@@ -357,6 +384,15 @@ class LbmSolver:
         return Stats(s.avg_density, s.min_density, s.max_density, s.avg_speed, s.max_speed, s.force_x, s.force_y,
                      s.force_z, s.max_stress, bool(s.has_nan), bool(s.valid), s.total_mass, tuple(s.force_sum),
                      int(s.fluid_cells), {"density_sum": s.density_sum, "speed_sum": s.speed_sum})
+
+    def AerodynamicForces(self) -> AerodynamicForces:
+        """FieldOverlay::ComputeAerodynamicForces (FieldOverlay.cpp:469-621) of
+        the current state, integrated on the device in FP64 (no field readback)."""
+        a = _AeroForces()
+        self._check(self._lib.fc_lbm_aero_forces(self._h, ctypes.byref(a)), "AerodynamicForces")
+        return AerodynamicForces(a.force[0], a.force[1], a.force[2], a.min_stress, a.max_stress,
+                                 tuple(a.center_of_pressure), tuple(a.lift_arrow_base), bool(a.has_nan),
+                                 tuple(a.force_sum), a.lift_weight_sum, a.force_weight_sum, int(a.solid_cells))
 
     def ProbeSliceHealth(self, zLayer: int) -> bool:
         d = ctypes.c_int32()

@@ -118,6 +118,20 @@ typedef struct fc_stats {
     uint64_t fluid_cells;
 } fc_stats;
 
+/* FieldOverlay::AerodynamicForces (FieldOverlay.h:186-195) plus the FP64
+ * sums behind it. */
+typedef struct fc_aero_forces {
+    float force[3];              /* forceX/Y/Z: the FP64 sums rounded to float */
+    float min_stress, max_stress;
+    float center_of_pressure[3]; /* world units */
+    float lift_arrow_base[3];
+    int32_t has_nan;
+    double force_sum[3];         /* FP64 surface integral of the momentum-exchange force */
+    double lift_weight_sum;      /* sum of |Fz| over solid cells */
+    double force_weight_sum;     /* sum of |F| over solid cells */
+    uint64_t solid_cells;
+} fc_aero_forces;
+
 typedef struct fc_lbm fc_lbm;
 
 /* Allocates an empty solver object (no device work). Pair with destroy. */
@@ -208,6 +222,16 @@ FC_LBM_API int fc_lbm_launch_count(const fc_lbm* h, uint64_t* launches);
 FC_LBM_API int fc_lbm_save_populations(fc_lbm* h, float* out, size_t count);
 /* Restores a state written by fc_lbm_save_populations (Q*N floats). */
 FC_LBM_API int fc_lbm_load_populations(fc_lbm* h, const float* in, size_t count);
+
+/* FieldOverlay::ComputeAerodynamicForces (FieldOverlay.cpp:469-621) on the
+ * current state, without the 4-float-per-cell field readback it takes in the
+ * reference: the solid cells' momentum-exchange forces (the field's solid
+ * entries) are summed on the device in FP64, the centre of pressure is the
+ * |Fz|-weighted mean cell centre (|F|-weighted, then geometric, when the
+ * weights vanish), and the lift arrow's base sits one cell above the top skin
+ * in a 5x5 column patch around it. World positions use the grid's cell size
+ * and origin from fc_lbm_init. Blocking. */
+FC_LBM_API int fc_lbm_aero_forces(fc_lbm* h, fc_aero_forces* out);
 
 /* Statistics of a population set computed without allocating anything: no
  * cudaMalloc, cudaFree or allocating library call happens inside. This entry

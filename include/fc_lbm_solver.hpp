@@ -138,6 +138,15 @@ public:
         fc_lbm_probe_slice_health(h_, zLayer, &d);
         return d != 0;
     }
+    // FieldOverlay::ComputeAerodynamicForces (FieldOverlay.cpp:469-621) of the
+    // current state, integrated on the device in FP64. The returned struct
+    // has the reference's fields plus the FP64 sums; `ok` false on failure.
+    fc_aero_forces AerodynamicForces(bool* ok = nullptr) {
+        fc_aero_forces a{};
+        const int rc = fc_lbm_aero_forces(h_, &a);
+        if (ok) *ok = rc == FC_LBM_OK;
+        return a;
+    }
     // LbmReference::HasDiverged (LbmReference.h:129), a device flag here.
     bool HasDiverged() {
         int32_t d = 0;

@@ -286,3 +286,93 @@ def voxelize_reference(positions, indices, target_resolution=640, padding=(0.3, 
     lib.ref_voxels_copy(h, solid.ctypes.data, sdf.ctypes.data)
     lib.ref_voxels_free(h)
     return (nx, ny, nz), float(cell[0]), origin, solid.reshape(nz, ny, nx), sdf.reshape(nz, ny, nx)
+
+
+# ---- aerodynamic forces (FieldOverlay::ComputeAerodynamicForces) ----
+def aero_forces(solid, field, cell_size=1.0, origin=(0.0, 0.0, 0.0)) -> dict:
+    """Restatement of FieldOverlay::ComputeAerodynamicForces
+    (FlowCraft/FieldOverlay.cpp:469-621) over a 4-float-per-cell field:
+    FP64 sums of the solid cells' momentum-exchange force, the lift-weighted
+    (|Fz|) centre of pressure with the force-weighted and geometric
+    fallbacks, the stress range over loaded skin cells and the lift arrow's
+    base above the top skin. The sums are float64 like the reference's; their
+    order differs (numpy pairwise), so results agree to rounding."""
+    solid = np.asarray(solid, dtype=np.uint8)
+    nz, ny, nx = solid.shape
+    f = np.asarray(field, dtype=np.float32).reshape(nz, ny, nx, 4)
+    zz, yy, xx = np.nonzero(solid)
+    cs = np.float32(cell_size)
+    org = np.asarray(origin, dtype=np.float32)
+    # VoxelGrid::CellCenter in float: world x from grid y, world y from grid x
+    px = (org[0] + (yy.astype(np.float32) + np.float32(0.5)) * cs).astype(np.float64)
+    py = (org[1] + (xx.astype(np.float32) + np.float32(0.5)) * cs).astype(np.float64)
+    pz = (org[2] + (zz.astype(np.float32) + np.float32(0.5)) * cs).astype(np.float64)
+    v = f[zz, yy, xx]
+    finite = np.isfinite(v).all(axis=1)
+    out = {"has_nan": bool((~finite).any())}
+    v64 = v[finite].astype(np.float64)
+    fx, fy, fz = v64[:, 1], v64[:, 2], v64[:, 3]
+    pxf, pyf, pzf = px[finite], py[finite], pz[finite]
+    out["force_sum"] = (fx.sum(), fy.sum(), fz.sum())
+    out["force"] = tuple(float(np.float32(s)) for s in out["force_sum"])
+    wl = np.abs(fz)
+    wf = np.sqrt(fx * fx + fy * fy + fz * fz)
+    stress = v[finite][:, 0]
+    loaded = stress[stress > 0]
+    hi = float(loaded.max()) if loaded.size else None
+    out["min_stress"] = 0.0
+    out["max_stress"] = float(np.float32(1e-6)) if hi is None else (hi if hi > 0.0 else float(np.float32(1e-6)))
+    if wl.sum() > 1e-9:
+        s = wl.sum()
+        cp = ((wl * pxf).sum() / s, (wl * pyf).sum() / s, (wl * pzf).sum() / s)
+    elif wf.sum() > 1e-9:
+        s = wf.sum()
+        cp = ((wf * pxf).sum() / s, (wf * pyf).sum() / s, (wf * pzf).sum() / s)
+    elif zz.size:
+        cp = (px.mean(), py.mean(), pz.mean())
+    else:
+        cp = (0.0, 0.0, 0.0)
+    cp = np.asarray(cp, dtype=np.float64).astype(np.float32)
+    out["center_of_pressure"] = tuple(float(c) for c in cp)
+    out["lift_weight_sum"] = float(wl.sum())
+    out["force_weight_sum"] = float(wf.sum())
+    out["solid_cells"] = int(zz.size)
+    gx = int(np.clip(np.floor((cp[1] - org[1]) / cs), 0, max(nx - 1, 0)))
+    gy = int(np.clip(np.floor((cp[0] - org[0]) / cs), 0, max(ny - 1, 0)))
+    top = -1
+    for dy in range(-2, 3):
+        y = int(np.clip(gy + dy, 0, max(ny - 1, 0)))
+        for dx in range(-2, 3):
+            x = int(np.clip(gx + dx, 0, max(nx - 1, 0)))
+            col = np.nonzero(solid[:, y, x])[0]
+            if col.size:
+                top = max(top, int(col.max()))
+    eff = top if top >= 0 else max(int(zz.max()) if zz.size else -1, 0)
+    out["lift_arrow_base"] = (out["center_of_pressure"][0], out["center_of_pressure"][1],
+                              float(org[2] + (np.float32(eff) + np.float32(1.0)) * cs))
+    return out
+
+
+class _RefAero(ctypes.Structure):
+    _fields_ = [("force", ctypes.c_float * 3), ("min_stress", ctypes.c_float), ("max_stress", ctypes.c_float),
+                ("center_of_pressure", ctypes.c_float * 3), ("lift_arrow_base", ctypes.c_float * 3),
+                ("has_nan", ctypes.c_int32)]
+
+
+def aero_forces_reference(solid, field, cell_size=1.0, origin=(0.0, 0.0, 0.0)) -> dict:
+    """FlowCraft's own FieldOverlay::ComputeAerodynamicForces (oracle/_ref)."""
+    lib = _vox_lib("ref")
+    if not hasattr(lib, "_aero_bound"):
+        lib.ref_aero_forces.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(_RefAero)]
+        lib._aero_bound = True
+    solid = np.ascontiguousarray(solid, dtype=np.uint8)
+    nz, ny, nx = solid.shape
+    field = np.ascontiguousarray(field, dtype=np.float32)
+    org = np.ascontiguousarray(origin, dtype=np.float32)
+    r = _RefAero()
+    lib.ref_aero_forces(nx, ny, nz, float(cell_size), org.ctypes.data, solid.ctypes.data, field.ctypes.data,
+                        ctypes.byref(r))
+    return {"force": tuple(r.force), "min_stress": r.min_stress, "max_stress": r.max_stress,
+            "center_of_pressure": tuple(r.center_of_pressure), "lift_arrow_base": tuple(r.lift_arrow_base),
+            "has_nan": bool(r.has_nan)}

@@ -145,3 +145,43 @@ void ref_voxels_copy(const ref_voxels* v, uint8_t* solid, float* sdf) {
 void ref_voxels_free(ref_voxels* v) { delete v; }
 
 }  // extern "C"
+
+// ---- FieldOverlay::ComputeAerodynamicForces (FlowCraft/FieldOverlay.cpp:469-621) ----
+#include "FieldOverlay.h"
+
+extern "C" {
+
+struct ref_aero {
+    float force[3];
+    float min_stress, max_stress;
+    float center_of_pressure[3];
+    float lift_arrow_base[3];
+    int32_t has_nan;
+};
+
+void ref_aero_forces(int nx, int ny, int nz, float cell_size, const float* origin, const uint8_t* solid,
+                     const float* field, ref_aero* out) {
+    VoxelGrid grid;
+    grid.nx = nx;
+    grid.ny = ny;
+    grid.nz = nz;
+    grid.cellSize = cell_size;
+    grid.origin = Vec3(origin[0], origin[1], origin[2]);
+    grid.solid.assign(solid, solid + grid.CellCount());
+    std::vector<float> f(field, field + grid.CellCount() * 4);
+    FieldOverlay::AerodynamicForces a = FieldOverlay::ComputeAerodynamicForces(grid, f);
+    out->force[0] = a.forceX;
+    out->force[1] = a.forceY;
+    out->force[2] = a.forceZ;
+    out->min_stress = a.minStress;
+    out->max_stress = a.maxStress;
+    out->center_of_pressure[0] = a.centerOfPressure.x;
+    out->center_of_pressure[1] = a.centerOfPressure.y;
+    out->center_of_pressure[2] = a.centerOfPressure.z;
+    out->lift_arrow_base[0] = a.liftArrowBase.x;
+    out->lift_arrow_base[1] = a.liftArrowBase.y;
+    out->lift_arrow_base[2] = a.liftArrowBase.z;
+    out->has_nan = a.hasNaN ? 1 : 0;
+}
+
+}  // extern "C"
