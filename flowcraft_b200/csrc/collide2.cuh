@@ -52,9 +52,16 @@ __device__ __forceinline__ float2 edotu2(float2 ux, float2 uy, float2 uz) {
     return s;
 }
 
-// Offset-space collision (collide_offsets) for two cells with FFMA2.
+// Moments and Pi_neq of two cells, the first half of the offset-space
+// collision: everything the relaxation needs once the populations are spent.
+struct Mom2 {
+    float2 drho, rho, inv, ux, uy, uz, u2;
+    float2 pxx, pyy, pzz, pxy, pxz, pyz, pp;  // Pi_neq and Pi:Pi
+};
+
+// Returns the two-bit divergence mask (bit 0: cell A, bit 1: cell B).
 template <int Q>
-__device__ __forceinline__ unsigned collide_offsets2(float2 (&h)[Q], float tau, float cs) {
+__device__ __forceinline__ unsigned moments2(const float2 (&h)[Q], Mom2& mo) {
     using L = Lattice<Q>;
     constexpr int NP = (Q - 1) / 2;
     constexpr float si = 1.0f / 256.0f;
@@ -87,14 +94,14 @@ __device__ __forceinline__ unsigned collide_offsets2(float2 (&h)[Q], float tau, 
         if constexpr (Y * Z > 0) syz = add2(syz, sp[k]);
         if constexpr (Y * Z < 0) syz = sub2(syz, sp[k]);
     });
-    const float2 drho = mul2(m, bc2(si));
-    const float2 rho = add2(bc2(1.0f), drho);
-    float2 inv;
-    inv.x = rho.x > 1e-6f ? __fdividef(1.0f, rho.x) : 1.0f;
-    inv.y = rho.y > 1e-6f ? __fdividef(1.0f, rho.y) : 1.0f;
-    const float2 isi = mul2(inv, bc2(si));
-    const float2 ux = mul2(jx, isi), uy = mul2(jy, isi), uz = mul2(jz, isi);
-    const float2 u2 = fma2(ux, ux, fma2(uy, uy, mul2(uz, uz)));
+    mo.drho = mul2(m, bc2(si));
+    mo.rho = add2(bc2(1.0f), mo.drho);
+    mo.inv.x = mo.rho.x > 1e-6f ? __fdividef(1.0f, mo.rho.x) : 1.0f;
+    mo.inv.y = mo.rho.y > 1e-6f ? __fdividef(1.0f, mo.rho.y) : 1.0f;
+    const float2 isi = mul2(mo.inv, bc2(si));
+    mo.ux = mul2(jx, isi), mo.uy = mul2(jy, isi), mo.uz = mul2(jz, isi);
+    mo.u2 = fma2(mo.ux, mo.ux, fma2(mo.uy, mo.uy, mul2(mo.uz, mo.uz)));
+    const float2 rho = mo.rho, u2 = mo.u2;
     // bit 0: cell A trips the divergence test, bit 1: cell B
     const unsigned bad = (rho.x > 0.0f && rho.x < __int_as_float(0x7f800000) && u2.x <= 4.0f ? 0u : 1u) |
                          (rho.y > 0.0f && rho.y < __int_as_float(0x7f800000) && u2.y <= 4.0f ? 0u : 2u);
@@ -102,32 +109,40 @@ __device__ __forceinline__ unsigned collide_offsets2(float2 (&h)[Q], float tau, 
     // Pi_neq = 2^-8 S - drho/3 I - rho u u, with the negations folded into
     // constants so every step is one FFMA2 / FMUL2
     constexpr float third = 1.0f / 3.0f;
-    const float2 nd3 = mul2(drho, bc2(-third));
+    const float2 nd3 = mul2(mo.drho, bc2(-third));
     const float2 nrho = mul2(rho, bc2(-1.0f));
-    const float2 nrux = mul2(nrho, ux), nruy = mul2(nrho, uy);
-    const float2 pxx = fma2(nrux, ux, fma2(sxx, bc2(si), nd3));
-    const float2 pyy = fma2(nruy, uy, fma2(syy, bc2(si), nd3));
-    const float2 pzz = fma2(mul2(nrho, uz), uz, fma2(szz, bc2(si), nd3));
-    const float2 pxy = fma2(nrux, uy, mul2(sxy, bc2(si)));
-    const float2 pxz = fma2(nrux, uz, mul2(sxz, bc2(si)));
-    const float2 pyz = fma2(nruy, uz, mul2(syz, bc2(si)));
+    const float2 nrux = mul2(nrho, mo.ux), nruy = mul2(nrho, mo.uy);
+    mo.pxx = fma2(nrux, mo.ux, fma2(sxx, bc2(si), nd3));
+    mo.pyy = fma2(nruy, mo.uy, fma2(syy, bc2(si), nd3));
+    mo.pzz = fma2(mul2(nrho, mo.uz), mo.uz, fma2(szz, bc2(si), nd3));
+    mo.pxy = fma2(nrux, mo.uy, mul2(sxy, bc2(si)));
+    mo.pxz = fma2(nrux, mo.uz, mul2(sxz, bc2(si)));
+    mo.pyz = fma2(nruy, mo.uz, mul2(syz, bc2(si)));
+    const float2 off = fma2(mo.pxy, mo.pxy, fma2(mo.pxz, mo.pxz, mul2(mo.pyz, mo.pyz)));
+    mo.pp = fma2(mo.pxx, mo.pxx, fma2(mo.pyy, mo.pyy, fma2(mo.pzz, mo.pzz, mul2(bc2(2.0f), off))));
+    return bad;
+}
 
-    const float2 off = fma2(pxy, pxy, fma2(pxz, pxz, mul2(pyz, pyz)));
-    const float2 pp = fma2(pxx, pxx, fma2(pyy, pyy, fma2(pzz, pzz, mul2(bc2(2.0f), off))));
-    float2 g;
-    {
-        const float k0 = (18.0f * 1.41421356f) * cs * cs;
-        const float tt = tau * tau;
-        float pim = pp.x > 0.0f ? pp.x * rsqrtf(pp.x) : 0.0f;
-        float t2 = fmaf(k0, pim * (rho.x < 1e-6f ? 1e6f : inv.x), tt);
-        g.x = (1.0f - __fdividef(2.0f, tau + t2 * rsqrtf(t2))) * 4.5f;
-        pim = pp.y > 0.0f ? pp.y * rsqrtf(pp.y) : 0.0f;
-        t2 = fmaf(k0, pim * (rho.y < 1e-6f ? 1e6f : inv.y), tt);
-        g.y = (1.0f - __fdividef(2.0f, tau + t2 * rsqrtf(t2))) * 4.5f;
-    }
+// Relaxation factor g = (1 - 1/tau_eff) * 4.5 of one cell under the
+// Smagorinsky closure, tau_eff = (tau + sqrt(tau^2 + 18 sqrt2 Cs^2 |Pi|/rho))/2
+// (LbmReference.cpp:439-444).
+__device__ __forceinline__ float smagorinsky_g(float pp, float rho, float inv, float tau, float cs) {
+    const float k0 = (18.0f * 1.41421356f) * cs * cs;
+    const float pim = pp > 0.0f ? pp * rsqrtf(pp) : 0.0f;
+    const float t2 = fmaf(k0, pim * (rho < 1e-6f ? 1e6f : inv), tau * tau);
+    return (1.0f - __fdividef(2.0f, tau + t2 * rsqrtf(t2))) * 4.5f;
+}
 
-    const float2 ntr3 = mul2(add2(add2(pxx, pyy), pzz), bc2(-third));  // -tr/3
-    const float2 a = fma2(mul2(bc2(-1.5f), rho), u2, drho);            // drho - 1.5 rho u^2
+// Second half: post-collision offsets of both cells from their moments and
+// relaxation factors g.
+template <int Q>
+__device__ __forceinline__ void relax2(float2 (&h)[Q], const Mom2& mo, float2 g) {
+    using L = Lattice<Q>;
+    constexpr int NP = (Q - 1) / 2;
+    constexpr float third = 1.0f / 3.0f;
+    const float2 rho = mo.rho;
+    const float2 ntr3 = mul2(add2(add2(mo.pxx, mo.pyy), mo.pzz), bc2(-third));  // -tr/3
+    const float2 a = fma2(mul2(bc2(-1.5f), rho), mo.u2, mo.drho);              // drho - 1.5 rho u^2
     h[0] = mul2(bc2(256.0f * L::w(0)), fma2(g, ntr3, a));
     static_for<0, NP>([&](auto P) {
         constexpr int i = 2 * decltype(P)::value + 1;
@@ -136,21 +151,31 @@ __device__ __forceinline__ unsigned collide_offsets2(float2 (&h)[Q], float tau, 
         constexpr int X = L::ex(i), Y = L::ey(i), Z = L::ez(i);
         constexpr float ws = 256.0f * L::w(i);
         constexpr bool flip = !lead_positive<Q>(i);  // then o leads positive
-        const float2 eu = edotu2<Q, flip ? o : i>(ux, uy, uz);
+        const float2 eu = edotu2<Q, flip ? o : i>(mo.ux, mo.uy, mo.uz);
         const float2 re = mul2(rho, eu);
         const float2 base = fma2(mul2(bc2(4.5f), re), eu, a);
         float2 qp = ntr3;
-        if constexpr (X != 0) qp = add2(qp, pxx);
-        if constexpr (Y != 0) qp = add2(qp, pyy);
-        if constexpr (Z != 0) qp = add2(qp, pzz);
-        if constexpr (X * Y != 0) qp = fma2(bc2(2.0f * (float)(X * Y)), pxy, qp);
-        if constexpr (X * Z != 0) qp = fma2(bc2(2.0f * (float)(X * Z)), pxz, qp);
-        if constexpr (Y * Z != 0) qp = fma2(bc2(2.0f * (float)(Y * Z)), pyz, qp);
+        if constexpr (X != 0) qp = add2(qp, mo.pxx);
+        if constexpr (Y != 0) qp = add2(qp, mo.pyy);
+        if constexpr (Z != 0) qp = add2(qp, mo.pzz);
+        if constexpr (X * Y != 0) qp = fma2(bc2(2.0f * (float)(X * Y)), mo.pxy, qp);
+        if constexpr (X * Z != 0) qp = fma2(bc2(2.0f * (float)(X * Z)), mo.pxz, qp);
+        if constexpr (Y * Z != 0) qp = fma2(bc2(2.0f * (float)(Y * Z)), mo.pyz, qp);
         const float2 r = mul2(bc2(ws), fma2(g, qp, base));
         const float2 s = mul2(bc2(3.0f * ws), re);
         h[flip ? o : i] = add2(r, s);
         h[flip ? i : o] = sub2(r, s);
     });
+}
+
+// Offset-space collision (collide_offsets) for two cells with FFMA2.
+template <int Q>
+__device__ __forceinline__ unsigned collide_offsets2(float2 (&h)[Q], float tau, float cs) {
+    Mom2 mo;
+    const unsigned bad = moments2<Q>(h, mo);
+    const float2 g = make_float2(smagorinsky_g(mo.pp.x, mo.rho.x, mo.inv.x, tau, cs),
+                                 smagorinsky_g(mo.pp.y, mo.rho.y, mo.inv.y, tau, cs));
+    relax2<Q>(h, mo, g);
     return bad;
 }
 

@@ -53,6 +53,10 @@ struct fc_lbm {
     double* d_aero_result = nullptr;
     float cell_size = 1.0f;
     float origin[3] = {0.0f, 0.0f, 0.0f};
+    bool closure_on = false;  // learned closure in place of Smagorinsky
+    fc::ClosureDev closure{};
+    uint4* d_closure = nullptr;
+    uint8_t* d_wall = nullptr;
     float* d_stage = nullptr;
     float* h_stage = nullptr;
     size_t stage_floats = 0;
@@ -182,6 +186,9 @@ void release(fc_lbm* h) {
     dfree(h->d_stats_result);
     dfree(h->d_aero_partials);
     dfree(h->d_aero_result);
+    dfree(h->d_closure);
+    dfree(h->d_wall);
+    h->closure_on = false;
     dfree(h->d_stage);
     if (h->h_stage) cudaFreeHost(h->h_stage);
     h->h_stage = nullptr;
@@ -312,6 +319,24 @@ int leave_stream(fc_lbm* h, cudaStream_t s) {
     return FC_LBM_OK;
 }
 
+// The two step kernels, with or without the learned closure.
+cudaError_t launch_bulk(fc_lbm* h, const fc::StepParams& p, const void* fin, void* fout, int z0, int zc,
+                        cudaStream_t s, int* nl) {
+    if (h->closure_on)
+        return fc::launch_bulk_pull_learned(h->q, h->storage, fin, fout, h->d_bulk_bits, h->g, p, z0, zc,
+                                            h->d_diverged, s, nl, h->closure);
+    return fc::launch_bulk_pull(h->q, h->storage, fin, fout, h->d_bulk_bits, h->g, p, z0, zc, h->d_diverged, s, nl);
+}
+
+cudaError_t launch_boundary(fc_lbm* h, const fc::StepParams& p, const void* fin, void* fout, uint32_t b, uint32_t e,
+                            cudaStream_t s) {
+    const fc::BoundaryList bl{h->d_cells, h->d_links, h->d_coef_off, h->d_coef};
+    if (h->closure_on)
+        return fc::launch_boundary_pull_learned(h->q, h->storage, fin, fout, bl, b, e, h->g, p, h->d_diverged, s,
+                                                h->closure);
+    return fc::launch_boundary_pull(h->q, h->storage, fin, fout, bl, b, e, h->g, p, h->d_diverged, s);
+}
+
 int step_range_on(fc_lbm* h, cudaStream_t s, int z0, int zc) {
     const int z1 = std::min(h->g.nz, z0 + zc);
     z0 = std::max(0, z0);
@@ -321,16 +346,12 @@ int step_range_on(fc_lbm* h, cudaStream_t s, int z0, int zc) {
     void* fout = h->pop[1 - h->cur];
     if (h->n_bulk > 0) {
         int nl = 0;
-        FC_TRY(h, fc::launch_bulk_pull(h->q, h->storage, fin, fout, h->d_bulk_bits, h->g, p, z0, z1 - z0,
-                                       h->d_diverged, s, &nl),
-               "bulk step");
+        FC_TRY(h, launch_bulk(h, p, fin, fout, z0, z1 - z0, s, &nl), "bulk step");
         h->launches += nl;
     }
     const uint32_t b = h->z_begin[(size_t)z0], e = h->z_begin[(size_t)z1];
     if (e > b) {
-        fc::BoundaryList bl{h->d_cells, h->d_links, h->d_coef_off, h->d_coef};
-        FC_TRY(h, fc::launch_boundary_pull(h->q, h->storage, fin, fout, bl, b, e, h->g, p, h->d_diverged, s),
-               "boundary step");
+        FC_TRY(h, launch_boundary(h, p, fin, fout, b, e, s), "boundary step");
         h->launches++;
     }
     return FC_LBM_OK;
@@ -668,6 +689,108 @@ int fc_lbm_aero_forces(fc_lbm* h, fc_aero_forces* out) {
     return FC_LBM_OK;
 }
 
+int fc_lbm_set_closure(fc_lbm* h, const fc_closure* c) {
+    FC_RC(check_ready(h));
+    if (!c) {
+        h->closure_on = false;
+        return FC_LBM_OK;
+    }
+    if (h->storage == FC_STORAGE_FP32)
+        return fail(h, FC_LBM_ERR_UNSUPPORTED, "the learned closure runs on the FP16/BF16 offset storage formats");
+    if (h->g.nx % 2 != 0) return fail(h, FC_LBM_ERR_UNSUPPORTED, "the learned closure needs an even nx");
+    if (!c->w1 || !c->b1 || !c->w2 || !c->b2 || !c->w3)
+        return fail(h, FC_LBM_ERR_INVALID_ARG, "closure weights missing");
+    bool ok = std::isfinite(c->b3) && std::isfinite(c->out_scale) && c->out_scale > 0.0f &&
+              std::isfinite(c->filter_width);
+    for (int k = 0; k < FC_CLOSURE_INPUTS; ++k) ok = ok && std::isfinite(c->mean[k]) && c->std[k] > 0.0f;
+    for (int k = 0; k < 3; ++k) ok = ok && !(c->lo[k] > c->hi[k]);
+    const int H = FC_CLOSURE_HIDDEN;
+    for (int i = 0; i < FC_CLOSURE_INPUTS * H && ok; ++i) ok = std::isfinite(c->w1[i]);
+    for (int i = 0; i < H * H && ok; ++i) ok = std::isfinite(c->w2[i]);
+    for (int i = 0; i < H && ok; ++i)
+        ok = std::isfinite(c->b1[i]) && std::isfinite(c->b2[i]) && std::isfinite(c->w3[i]);
+    if (!ok)
+        return fail(h, FC_LBM_ERR_INVALID_ARG, "closure parameters must be finite, with std > 0 and out_scale > 0");
+    DeviceGuard dg(h->device);
+    if (!h->d_wall) {
+        uint8_t* tmp = nullptr;
+        FC_TRY(h, cudaMalloc(&h->d_wall, h->g.n), "alloc wall distance");
+        cudaError_t e = cudaMalloc(&tmp, h->g.n);
+        if (e == cudaSuccess) e = fc::launch_wall_distance(h->d_solid, h->g, h->d_wall, tmp, h->stream);
+        const int rc = e == cudaSuccess ? wait_stream(h, kTransferTimeoutMs) : cuda_fail(h, e, "wall distance");
+        if (tmp) cudaFree(tmp);
+        if (rc != FC_LBM_OK) {
+            dfree(h->d_wall);
+            return rc;
+        }
+    }
+    if (!h->d_closure) FC_TRY(h, cudaMalloc(&h->d_closure, fc::kClosureVec * sizeof(uint4)), "alloc closure");
+    std::vector<uint4> frag(fc::kClosureVec);
+    fc::pack_closure(c->w1, c->b1, c->w2, c->b2, c->w3, c->b3, c->out_scale, frag.data());
+    // ordered after any step already queued on the solver's stream
+    FC_TRY(h, cudaMemcpyAsync(h->d_closure, frag.data(), frag.size() * sizeof(uint4), cudaMemcpyHostToDevice,
+                              h->stream),
+           "upload closure");
+    FC_RC(wait_stream(h, kTransferTimeoutMs));
+    fc::ClosureDev cd{};
+    cd.frag = h->d_closure;
+    cd.wall = h->d_wall;
+    for (int k = 0; k < FC_CLOSURE_INPUTS; ++k) {
+        cd.mean[k] = c->mean[k];
+        cd.inv_std[k] = 1.0f / c->std[k];
+    }
+    for (int k = 0; k < 3; ++k) {
+        cd.lo[k] = c->lo[k];
+        cd.hi[k] = c->hi[k];
+    }
+    cd.filter_width = c->filter_width;
+    h->closure = cd;
+    h->closure_on = true;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_closure_probe(fc_lbm* h, float* out, uint8_t* in_range, size_t cells) {
+    FC_RC(check_ready(h));
+    if (!h->closure_on) return fail(h, FC_LBM_ERR_NOT_INITIALIZED, "no learned closure set");
+    if (!out || !in_range || cells != h->g.n) return FC_LBM_ERR_INVALID_ARG;
+    DeviceGuard dg(h->device);
+    float* d_out = nullptr;
+    uint8_t* d_rng = nullptr;
+    FC_TRY(h, cudaMalloc(&d_out, h->g.n * 5 * sizeof(float)), "alloc probe");
+    cudaError_t e = cudaMalloc(&d_rng, h->g.n);
+    if (e == cudaSuccess)
+        e = fc::launch_closure_probe(h->q, h->storage, h->pop[h->cur], h->g, h->closure, d_out, d_rng, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, d_out, h->g.n * 5 * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(in_range, d_rng, h->g.n, cudaMemcpyDeviceToHost, h->stream);
+    const int rc = e == cudaSuccess ? wait_stream(h, kTransferTimeoutMs) : cuda_fail(h, e, "closure probe");
+    cudaFree(d_out);
+    if (d_rng) cudaFree(d_rng);
+    h->launches++;
+    return rc;
+}
+
+int fc_lbm_wall_distance(fc_lbm* h, uint8_t* out, size_t cells) {
+    FC_RC(check_ready(h));
+    if (!out || cells != h->g.n) return FC_LBM_ERR_INVALID_ARG;
+    DeviceGuard dg(h->device);
+    uint8_t* d = h->d_wall;
+    uint8_t* own = nullptr;
+    uint8_t* tmp = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (!d) {
+        e = cudaMalloc(&own, h->g.n);
+        if (e == cudaSuccess) e = cudaMalloc(&tmp, h->g.n);
+        if (e == cudaSuccess) e = fc::launch_wall_distance(h->d_solid, h->g, own, tmp, h->stream);
+        d = own;
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, h->g.n, cudaMemcpyDeviceToHost, h->stream);
+    const int rc = e == cudaSuccess ? wait_stream(h, kTransferTimeoutMs) : cuda_fail(h, e, "wall distance");
+    if (own) cudaFree(own);
+    if (tmp) cudaFree(tmp);
+    return rc;
+}
+
 int fc_lbm_probe_slice_health(fc_lbm* h, int32_t z, int32_t* diverged) {
     FC_RC(check_ready(h));
     if (!diverged) return FC_LBM_ERR_INVALID_ARG;
@@ -775,7 +898,6 @@ int fc_lbm_step_timed(fc_lbm* h, int32_t n, float* total_ms, float* bulk_ms, flo
         }
     }
     const uint32_t b = h->z_begin[0], e = h->z_begin[(size_t)h->g.nz];
-    fc::BoundaryList bl{h->d_cells, h->d_links, h->d_coef_off, h->d_coef};
     int rc = FC_LBM_OK;
     cudaEventRecord(ev[0], h->stream);
     for (int k = 0; k < n && rc == FC_LBM_OK; ++k) {
@@ -786,14 +908,13 @@ int fc_lbm_step_timed(fc_lbm* h, int32_t n, float* total_ms, float* bulk_ms, flo
         cudaError_t ce = cudaSuccess;
         if (h->n_bulk > 0) {
             int nl = 0;
-            ce = fc::launch_bulk_pull(h->q, h->storage, fin, fout, h->d_bulk_bits, h->g, p, 0, h->g.nz, h->d_diverged,
-                                      h->stream, &nl);
+            ce = launch_bulk(h, p, fin, fout, 0, h->g.nz, h->stream, &nl);
             h->launches += nl;
         }
         cudaEventRecord(ev[3 + 4 * k], h->stream);
         cudaEventRecord(ev[4 + 4 * k], h->stream);
         if (ce == cudaSuccess && e > b) {
-            ce = fc::launch_boundary_pull(h->q, h->storage, fin, fout, bl, b, e, h->g, p, h->d_diverged, h->stream);
+            ce = launch_boundary(h, p, fin, fout, b, e, h->stream);
             h->launches++;
         }
         cudaEventRecord(ev[5 + 4 * k], h->stream);

@@ -77,9 +77,48 @@ struct BoundaryList {
 // storage: 0 fp32, 1 fp16 offset, 2 bf16 offset; q: 15 or 19.
 // Bulk cells of z range [z0, z0+zc): interior + shell kernels. *launched
 // receives the number of kernels enqueued (0..2).
+// Learned closure (closure.cuh): fragment-ordered weights, the per-cell wall
+// distance and the input normalization, passed to the kernels by value.
+constexpr int kClosureIn = 5;
+constexpr int kClosureHidden = 32;
+// 8 groups of 4 words per lane, 32 lanes (fragment order, pack_closure):
+//   0 W1 with b1 as the row of K slot 5 (n-tiles 0-3)   1 b2 as a K = 8
+//   fragment row (n-tiles 0-3)   2-5 W2 (one group per n-tile: k0 b0, k0 b1,
+//   k1 b0, k1 b1)   6 W3 (k0 b0, k0 b1, k1 b0, k1 b1)   7 b3 (word 0, FP32)
+constexpr int kClosureGroups = 8;
+constexpr int kClosureVec = kClosureGroups * 32;  // uint4 entries
+constexpr int kWallFar = 255;                     // wall-distance byte for 15.94+ cells
+
+struct ClosureDev {
+    const uint4* frag;    // kClosureVec entries
+    const uint8_t* wall;  // per-cell wall distance, 1/16-cell steps
+    float mean[kClosureIn];
+    float inv_std[kClosureIn];
+    float lo[3], hi[3];   // training range of inputs 0-2 (fallback outside)
+    float filter_width;   // input 4
+};
+
+// Host: packs FP32 weights (w1 [5][32], b1 [32], w2 [32][32], b2 [32], w3 [32],
+// b3; input-major, nu_t = relu(z) * out_scale) into kClosureVec fragment-ordered
+// entries: BF16 weights and hidden-layer biases, FP32 output bias.
+void pack_closure(const float* w1, const float* b1, const float* w2, const float* b2, const float* w3, float b3,
+                  float out_scale, uint4* out);
+// Chamfer distance (in 1/16 cells, capped at kWallFar) from every cell to the
+// nearest solid cell; `tmp` is a scratch array of g.n bytes.
+cudaError_t launch_wall_distance(const uint8_t* solid, const Geom& g, uint8_t* out, uint8_t* tmp, cudaStream_t s);
+
+cudaError_t launch_bulk_pull_learned(int q, int storage, const void* fin, void* fout, const uint32_t* bulk_bits,
+                                     const Geom& g, const StepParams& p, int z0, int zc, int* diverged,
+                                     cudaStream_t s, int* launched, const ClosureDev& cl);
+cudaError_t launch_closure_probe(int q, int storage, const void* f, const Geom& g, const ClosureDev& cl, float* out,
+                                 uint8_t* in_range, cudaStream_t s);
+
 cudaError_t launch_bulk_pull(int q, int storage, const void* fin, void* fout, const uint32_t* bulk_bits,
                              const Geom& g, const StepParams& p, int z0, int zc, int* diverged, cudaStream_t s,
                              int* launched);
+cudaError_t launch_boundary_pull_learned(int q, int storage, const void* fin, void* fout, const BoundaryList& bl,
+                                         uint32_t begin, uint32_t end, const Geom& g, const StepParams& p,
+                                         int* diverged, cudaStream_t s, const ClosureDev& cl);
 cudaError_t launch_boundary_pull(int q, int storage, const void* fin, void* fout, const BoundaryList& bl,
                                  uint32_t begin, uint32_t end, const Geom& g, const StepParams& p, int* diverged,
                                  cudaStream_t s);

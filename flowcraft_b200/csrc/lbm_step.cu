@@ -20,6 +20,7 @@
 //
 // Both kernels read one population set and write the other (ping-pong), so
 // they are independent and touch disjoint cells.
+#include "closure.cuh"
 #include "collide.cuh"
 #include "collide2.cuh"
 #include "lbm_internal.h"
@@ -375,6 +376,159 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs(const typename
     });
 }
 
+// k_bulk_pairs with the learned closure (16-bit offset storage). The MLP is a
+// warp-wide tensor-core operation, so no lane leaves before it: lanes without
+// a bulk pair run it on zero offsets and store nothing. Loads and stores are
+// those of k_bulk_pairs (aligned pair loads in interior warps for full pairs,
+// the general masked path otherwise); between them the collision runs in two
+// halves around the closure (moments2, closure_warp_mlp, relax2). Warps never
+// wait for one another: the closure's shared memory is private to each warp.
+template <int Q, class S>
+__global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned(const typename S::T* __restrict__ fin,
+                                                                        typename S::T* __restrict__ fout,
+                                                                        const uint32_t* __restrict__ bulk_bits,
+                                                                        Geom g, StepParams p, PlanePtrs pp, int z0,
+                                                                        int* __restrict__ diverged, ClosureDev cl) {
+    static_assert(!S::kExact, "the learned closure runs on the 16-bit offset formats");
+    using L = Lattice<Q>;
+    using T = typename S::T;
+    __shared__ uint32_t s_in[kBulkRows][32 * 8];
+    __shared__ float2 s_out[kBulkRows][32];
+    const int y = blockIdx.y * kBulkRows + threadIdx.y;
+    const int z = z0 + blockIdx.z;
+    if (y >= g.ny) return;  // the whole warp: one row
+    const size_t row = (size_t)z * g.ny + y;
+    const int k = 2 * threadIdx.x;
+    const int w = 2 * blockIdx.x + (k >> 5);
+    const uint32_t bits = w < g.wpr ? __ldg(bulk_bits + row * g.wpr + w) : 0u;
+    const int x = 64 * blockIdx.x + k;
+    unsigned pair = (bits >> (k & 31)) & 3u;
+    unsigned plane = 0;
+    if (x == 0) {
+        plane |= pair & 1u;
+        pair &= ~1u;
+    }
+    if (x + 1 == g.nx - 1) {
+        plane |= pair & 2u;
+        pair &= ~2u;
+    }
+    const uint32_t c = (uint32_t)(row * g.nx + x);
+    // both cells' wall distances in one aligned load (x and nx are even)
+    const unsigned wd = pair ? (unsigned)__ldg(reinterpret_cast<const unsigned short*>(cl.wall + c)) : 0xffffu;
+    const bool face = (y == 0) | (y == g.ny - 1) | (z == 0) | (z == g.nz - 1);
+    const bool edge = (blockIdx.x == 0) | (64 * (int)blockIdx.x + 64 >= g.nx);
+    if (plane) plane_cell<Q, S>(fin, fout, g, p, plane == 1u ? x : x + 1, plane == 1u ? c : (size_t)c + 1);
+    const bool va = pair & 1u, vb = pair & 2u;
+
+    // The load path is chosen per warp: the pure pair pull when every lane
+    // holds a full bulk pair or nothing, the masked general path otherwise.
+    // Lanes without a pair load from in-bounds addresses too (their own row)
+    // and store nothing, so neither path diverges.
+    const bool fast = !face && !edge && __all_sync(0xffffffffu, pair == 3u || pair == 0u);
+    const uint32_t cs = x < g.nx ? c : (uint32_t)(row * g.nx);
+    float2 v[Q];
+    if (fast) {
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            const T* src = static_cast<const T*>(pp.src[i]);
+            v[i] = L::ex(i) == 0 ? S::raw2(S::ld2(src + cs))
+                                 : make_float2(S::raw(S::ld(src + cs)), S::raw(S::ld(src + cs + 1u)));
+        });
+    } else {
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            const int py = y - L::ey(i), pz = z - L::ez(i);
+            const bool oy = py < 0 || py >= g.ny;
+            const bool oz = pz < 0 || pz >= g.nz;
+            const bool out = oy || oz;
+            const int pl = out ? edge_plane<Q, i>(oy, oz, p) : i;
+            const uint32_t off = out ? 0u : (uint32_t)link_offset<Q>(i, g);
+            const uint32_t sa = va ? c - off : cs;
+            const uint32_t sb = vb ? c + 1u - off : cs + 1u;
+            const T* base = fin + (size_t)pl * g.n;
+            v[i] = make_float2(S::raw(S::ld(base + sa)), S::raw(S::ld(base + sb)));
+        });
+    }
+    Mom2 mo;
+    const unsigned bad = moments2<Q>(v, mo) & pair;
+    // everything besides nu_t is settled before the MMA, so only the moments
+    // stay live across it
+    float xa0, xa1, xa2, xb0, xb1, xb2;
+    closure_invariants(mo.pxx.x, mo.pyy.x, mo.pzz.x, mo.pxy.x, mo.pxz.x, mo.pyz.x, mo.pp.x, mo.inv.x, xa0, xa1, xa2);
+    closure_invariants(mo.pxx.y, mo.pyy.y, mo.pzz.y, mo.pxy.y, mo.pxz.y, mo.pyz.y, mo.pp.y, mo.inv.y, xb0, xb1, xb2);
+    const bool la = closure_in_range(cl, xa0, xa1, xa2), lb = closure_in_range(cl, xb0, xb1, xb2);
+    const float sga = smagorinsky_g(mo.pp.x, mo.rho.x, mo.inv.x, p.tau, p.cs);
+    const float sgb = smagorinsky_g(mo.pp.y, mo.rho.y, mo.inv.y, p.tau, p.cs);
+    uint32_t* in = &s_in[threadIdx.y][threadIdx.x * 8];
+    closure_pack_inputs(cl, xa0, xa1, xa2, (float)(wd & 0xffu) * 0.0625f, in);
+    closure_pack_inputs(cl, xb0, xb1, xb2, (float)(wd >> 8) * 0.0625f, in + 4);
+    __syncwarp();
+    const float2 nu = closure_warp_mlp(cl.frag, s_in[threadIdx.y], s_out[threadIdx.y]);
+    if (!pair) return;
+    float2 gr;
+    gr.x = la ? (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.x, p.tau))) * 4.5f : sga;
+    gr.y = lb ? (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.y, p.tau))) * 4.5f : sgb;
+    relax2<Q>(v, mo, gr);
+    if (bad) atomicOr(diverged, 1);
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        T* dst = static_cast<T*>(pp.dst[i]);
+        const typename S::T2 hv = S::pack2(v[i].x, v[i].y);
+        if (pair == 3u) {
+            *reinterpret_cast<typename S::T2*>(dst + c) = hv;
+        } else {
+            if (va) dst[c] = hv.x;
+            if (vb) dst[c + 1u] = hv.y;
+        }
+    });
+}
+
+// The closure's inputs and nu_t for every cell of the current population set
+// as stored (no streaming): the same device code as the fused kernels, for
+// checking the inference against a CPU evaluation. Two cells per lane.
+// out[5*c .. 5*c+4] = inputs 0-3 and nu_t; in_range[c] = 1 when the learned
+// value is used.
+template <int Q, class S>
+__global__ void __launch_bounds__(128) k_closure_probe(const typename S::T* __restrict__ f, Geom g, ClosureDev cl,
+                                                       float* __restrict__ out, uint8_t* __restrict__ in_range) {
+    static_assert(!S::kExact, "the learned closure runs on the 16-bit offset formats");
+    __shared__ uint32_t s_in[4][32 * 8];
+    __shared__ float2 s_out[4][32];
+    const size_t c = 2 * ((size_t)blockIdx.x * blockDim.x + threadIdx.x);
+    const bool ha = c < g.n, hb = c + 1 < g.n;
+    float2 v[Q];
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        v[i] = make_float2(ha ? S::raw(S::ld(f + (size_t)i * g.n + c)) : 0.0f,
+                           hb ? S::raw(S::ld(f + (size_t)i * g.n + c + 1)) : 0.0f);
+    });
+    Mom2 mo;
+    moments2<Q>(v, mo);
+    float xa[4], xb[4];
+    closure_invariants(mo.pxx.x, mo.pyy.x, mo.pzz.x, mo.pxy.x, mo.pxz.x, mo.pyz.x, mo.pp.x, mo.inv.x, xa[0], xa[1],
+                       xa[2]);
+    closure_invariants(mo.pxx.y, mo.pyy.y, mo.pzz.y, mo.pxy.y, mo.pxz.y, mo.pyz.y, mo.pp.y, mo.inv.y, xb[0], xb[1],
+                       xb[2]);
+    xa[3] = ha ? (float)cl.wall[c] * 0.0625f : 0.0f;
+    xb[3] = hb ? (float)cl.wall[c + 1] * 0.0625f : 0.0f;
+    const int warp = threadIdx.x >> 5;
+    uint32_t* in = &s_in[warp][(threadIdx.x & 31) * 8];
+    closure_pack_inputs(cl, xa[0], xa[1], xa[2], xa[3], in);
+    closure_pack_inputs(cl, xb[0], xb[1], xb[2], xb[3], in + 4);
+    __syncwarp();
+    const float2 nu = closure_warp_mlp(cl.frag, s_in[warp], s_out[warp]);
+    if (ha) {
+        for (int k = 0; k < 4; ++k) out[5 * c + k] = xa[k];
+        out[5 * c + 4] = nu.x;
+        in_range[c] = closure_in_range(cl, xa[0], xa[1], xa[2]) ? 1 : 0;
+    }
+    if (hb) {
+        for (int k = 0; k < 4; ++k) out[5 * (c + 1) + k] = xb[k];
+        out[5 * (c + 1) + 4] = nu.y;
+        in_range[c + 1] = closure_in_range(cl, xb[0], xb[1], xb[2]) ? 1 : 0;
+    }
+}
+
 template <int Q, class S>
 __global__ void __launch_bounds__(32 * kBulkRows) k_bulk_shell(const typename S::T* __restrict__ fin,
                                                                 typename S::T* __restrict__ fout,
@@ -474,6 +628,93 @@ __global__ void __launch_bounds__(128) k_boundary_pull(const typename S::T* __re
     });
 }
 
+// k_boundary_pull with the learned closure (16-bit offset storage): the same
+// link handling in float populations, then the two-phase collision on
+// offsets (f - w) * 2^8 with the warp-wide closure. Every lane of a warp runs
+// the closure; only live fluid entries store.
+template <int Q, class S>
+__global__ void __launch_bounds__(128) k_boundary_pull_learned(const typename S::T* __restrict__ fin,
+                                                                typename S::T* __restrict__ fout, BoundaryList bl,
+                                                                uint32_t begin, uint32_t end, Geom g, StepParams p,
+                                                                int* __restrict__ diverged, ClosureDev cl) {
+    static_assert(!S::kExact, "the learned closure runs on the 16-bit offset formats");
+    using L = Lattice<Q>;
+    __shared__ uint32_t s_in[4][32 * 8];
+    __shared__ float2 s_out[4][32];
+    const uint32_t e = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = e < end;
+    const uint32_t c = live ? __ldg(bl.cells + e) : 0u;
+    const unsigned long long lk = live ? __ldg(bl.links + e) : 0ull;
+    const unsigned cls = (unsigned)(lk >> kClassShift) & 7u;
+    const bool fluid = live && cls != kCellSolidFill;
+    if (live && !fluid) {  // solid cell: f_i = w_i (LbmReference.cpp:264-267)
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            store_pop_c<Q, S, i>(fout, g.n, c, L::w(i));
+        });
+    }
+    const uint32_t nxy = (uint32_t)g.nxy;
+    const uint32_t z = c / nxy;
+    const uint32_t rem = c - z * nxy;
+    const uint32_t y = rem / (uint32_t)g.nx;
+    float2 h[Q];
+    if (fluid) {
+        const uint32_t co0 = __ldg(bl.coef_off + e);
+        uint32_t bzmask = 0;
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            if ((((unsigned)(lk >> (3 * i))) & 6u) == 2u) bzmask |= 1u << i;
+        });
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            constexpr int op = L::opp(i);
+            const unsigned kind = (unsigned)(lk >> (3 * i)) & 7u;
+            int pa = op;
+            size_t sa = c;
+            if (kind == kLinkStream) {
+                pa = i;
+                sa = (size_t)c - link_offset<Q>(i, g);
+            } else if (kind == kLinkEdge) {
+                const int py = (int)y - L::ey(i), pz = (int)z - L::ez(i);
+                pa = edge_plane<Q, i>(py < 0 || py >= g.ny, pz < 0 || pz >= g.nz, p);
+            }
+            const float va = load_plane<Q, S>(fin, pa, g.n, sa, L::w(i));
+            float v = va;
+            if (kind == kLinkBzNear || kind == kLinkBzFar) {
+                const float2 kk = __ldg(bl.coef + co0 + __popc(bzmask & ((1u << i) - 1u)));
+                const int pb = kind == kLinkBzNear ? op : i;
+                const size_t sb = kind == kLinkBzNear ? (size_t)c + link_offset<Q>(i, g) : (size_t)c;
+                const float vb = load_plane<Q, S>(fin, pb, g.n, sb, L::w(i));
+                v = kk.x * va + kk.y * vb;
+            }
+            h[i] = make_float2((v - L::w(i)) * 256.0f, 0.0f);
+        });
+    } else {
+        static_for<0, Q>([&](auto I) { h[decltype(I)::value] = make_float2(0.0f, 0.0f); });
+    }
+    Mom2 mo;
+    const unsigned bad = moments2<Q>(h, mo) & (fluid ? 1u : 0u);
+    float x0, x1, x2;
+    closure_invariants(mo.pxx.x, mo.pyy.x, mo.pzz.x, mo.pxy.x, mo.pxz.x, mo.pyz.x, mo.pp.x, mo.inv.x, x0, x1, x2);
+    const float x3 = fluid ? (float)__ldg(cl.wall + c) * 0.0625f : 0.0f;
+    const bool lin = closure_in_range(cl, x0, x1, x2);
+    const float sg = smagorinsky_g(mo.pp.x, mo.rho.x, mo.inv.x, p.tau, p.cs);
+    const int warp = threadIdx.x >> 5;
+    uint32_t* in = &s_in[warp][(threadIdx.x & 31) * 8];
+    closure_pack_inputs(cl, x0, x1, x2, x3, in);
+    closure_pack_inputs(cl, 0.0f, 0.0f, 0.0f, 0.0f, in + 4);
+    __syncwarp();
+    const float2 nu = closure_warp_mlp(cl.frag, s_in[warp], s_out[warp]);
+    if (!fluid) return;
+    const float gx = lin ? (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.x, p.tau))) * 4.5f : sg;
+    relax2<Q>(h, mo, make_float2(gx, gx));
+    if (bad) atomicOr(diverged, 1);
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        store_pop_c<Q, S, i>(fout, g.n, c, L::w(i) + h[i].x * (1.0f / 256.0f));
+    });
+}
+
 template <int Q, class S>
 static cudaError_t bulk_t(const void* fin, void* fout, const uint32_t* bits, const Geom& g, const StepParams& p,
                           int z0, int zc, int* dv, cudaStream_t s, int* launched) {
@@ -541,6 +782,61 @@ static cudaError_t boundary_t(const void* fin, void* fout, const BoundaryList& b
     return cudaGetLastError();
 }
 
+template <int Q, class S>
+static cudaError_t bulk_learned_t(const void* fin, void* fout, const uint32_t* bits, const Geom& g,
+                                  const StepParams& p, int z0, int zc, int* dv, cudaStream_t s, int* launched,
+                                  const ClosureDev& cl) {
+    *launched = 0;
+    if constexpr (S::kExact) {
+        return cudaErrorNotSupported;
+    } else {
+        if (zc <= 0) return cudaSuccess;
+        if (g.nx % 2 != 0) return cudaErrorNotSupported;
+        PlanePtrs pp{};
+        for (int i = 0; i < Q; ++i) {
+            const long long off = (long long)Lattice<Q>::ex(i) + (long long)Lattice<Q>::ey(i) * g.nx +
+                                  (long long)Lattice<Q>::ez(i) * g.nxy;
+            pp.src[i] = (const typename S::T*)fin + ((long long)i * (long long)g.n - off);
+            pp.dst[i] = (typename S::T*)fout + (size_t)i * g.n;
+        }
+        dim3 block(32, kBulkRows, 1);
+        dim3 grid((unsigned)((g.nx + 63) / 64), (unsigned)((g.ny + kBulkRows - 1) / kBulkRows), (unsigned)zc);
+        k_bulk_pairs_learned<Q, S><<<grid, block, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout, bits, g,
+                                                          p, pp, z0, dv, cl);
+        ++*launched;
+        return cudaGetLastError();
+    }
+}
+
+template <int Q, class S>
+static cudaError_t boundary_learned_t(const void* fin, void* fout, const BoundaryList& bl, uint32_t b, uint32_t e,
+                                      const Geom& g, const StepParams& p, int* dv, cudaStream_t s,
+                                      const ClosureDev& cl) {
+    if constexpr (S::kExact) {
+        return cudaErrorNotSupported;
+    } else {
+        if (e <= b) return cudaSuccess;
+        const unsigned threads = 128;
+        const unsigned blocks = (e - b + threads - 1) / threads;
+        k_boundary_pull_learned<Q, S><<<blocks, threads, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout, bl,
+                                                                 b, e, g, p, dv, cl);
+        return cudaGetLastError();
+    }
+}
+
+template <int Q, class S>
+static cudaError_t closure_probe_t(const void* f, const Geom& g, const ClosureDev& cl, float* out, uint8_t* in_range,
+                                   cudaStream_t s) {
+    if constexpr (S::kExact) {
+        return cudaErrorNotSupported;
+    } else {
+        const size_t pairs = (g.n + 1) / 2;
+        k_closure_probe<Q, S><<<(unsigned)((pairs + 127) / 128), 128, 0, s>>>((const typename S::T*)f, g, cl, out,
+                                                                              in_range);
+        return cudaGetLastError();
+    }
+}
+
 #define FC_DISPATCH(q, storage, FN, ...)                                              \
     do {                                                                              \
         if ((q) == 19) {                                                              \
@@ -565,6 +861,23 @@ cudaError_t launch_boundary_pull(int q, int storage, const void* fin, void* fout
                                  uint32_t begin, uint32_t end, const Geom& g, const StepParams& p, int* diverged,
                                  cudaStream_t s) {
     FC_DISPATCH(q, storage, boundary_t, fin, fout, bl, begin, end, g, p, diverged, s);
+}
+
+cudaError_t launch_bulk_pull_learned(int q, int storage, const void* fin, void* fout, const uint32_t* bulk_bits,
+                                     const Geom& g, const StepParams& p, int z0, int zc, int* diverged,
+                                     cudaStream_t s, int* launched, const ClosureDev& cl) {
+    FC_DISPATCH(q, storage, bulk_learned_t, fin, fout, bulk_bits, g, p, z0, zc, diverged, s, launched, cl);
+}
+
+cudaError_t launch_boundary_pull_learned(int q, int storage, const void* fin, void* fout, const BoundaryList& bl,
+                                         uint32_t begin, uint32_t end, const Geom& g, const StepParams& p,
+                                         int* diverged, cudaStream_t s, const ClosureDev& cl) {
+    FC_DISPATCH(q, storage, boundary_learned_t, fin, fout, bl, begin, end, g, p, diverged, s, cl);
+}
+
+cudaError_t launch_closure_probe(int q, int storage, const void* f, const Geom& g, const ClosureDev& cl, float* out,
+                                 uint8_t* in_range, cudaStream_t s) {
+    FC_DISPATCH(q, storage, closure_probe_t, f, g, cl, out, in_range, s);
 }
 
 }  // namespace fc

@@ -87,12 +87,21 @@ class _Stats(ctypes.Structure):
     ]
 
 
+_FPTR = ctypes.POINTER(ctypes.c_float)
+
+
 class _AeroForces(ctypes.Structure):
     _fields_ = [("force", ctypes.c_float * 3), ("min_stress", ctypes.c_float), ("max_stress", ctypes.c_float),
                 ("center_of_pressure", ctypes.c_float * 3), ("lift_arrow_base", ctypes.c_float * 3),
                 ("has_nan", ctypes.c_int32), ("force_sum", ctypes.c_double * 3),
                 ("lift_weight_sum", ctypes.c_double), ("force_weight_sum", ctypes.c_double),
                 ("solid_cells", ctypes.c_uint64)]
+
+
+class _Closure(ctypes.Structure):
+    _fields_ = [("w1", _FPTR), ("b1", _FPTR), ("w2", _FPTR), ("b2", _FPTR), ("w3", _FPTR), ("b3", ctypes.c_float),
+                ("out_scale", ctypes.c_float), ("mean", ctypes.c_float * 5), ("std", ctypes.c_float * 5),
+                ("lo", ctypes.c_float * 3), ("hi", ctypes.c_float * 3), ("filter_width", ctypes.c_float)]
 
 
 class _VoxelParams(ctypes.Structure):
@@ -137,6 +146,9 @@ SIGNATURES = {
     "fc_lbm_load_populations": (ctypes.c_int, [_P, _FP, _SZ]),
     "fc_lbm_stats_noalloc": (ctypes.c_int, [_P, _P, _P, _I32, _I32, _I32, _I32, _I32, _P, _P]),
     "fc_lbm_aero_forces": (ctypes.c_int, [_P, ctypes.POINTER(_AeroForces)]),
+    "fc_lbm_set_closure": (ctypes.c_int, [_P, ctypes.POINTER(_Closure)]),
+    "fc_lbm_closure_probe": (ctypes.c_int, [_P, _FP, ctypes.POINTER(ctypes.c_uint8), _SZ]),
+    "fc_lbm_wall_distance": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint8), _SZ]),
     "fc_lbm_voxel_grid": (ctypes.c_int, [_P, _SZ, ctypes.POINTER(_VoxelParams), _I32, _I32P, _FP, _FP, _P]),
     "fc_lbm_voxelize": (ctypes.c_int, [_P, _SZ, _P, _SZ, _I32P, ctypes.c_float, _FP, _I32, _P, _P, _P]),
 }
@@ -393,6 +405,46 @@ class LbmSolver:
         return AerodynamicForces(a.force[0], a.force[1], a.force[2], a.min_stress, a.max_stress,
                                  tuple(a.center_of_pressure), tuple(a.lift_arrow_base), bool(a.has_nan),
                                  tuple(a.force_sum), a.lift_weight_sum, a.force_weight_sum, int(a.solid_cells))
+
+    def SetClosure(self, weights) -> None:
+        """Installs a learned closure (flowcraft_b200.closure.ClosureWeights),
+        or returns to Smagorinsky with None. Raises LbmError when the storage
+        format or lattice cannot take it."""
+        if weights is None:
+            self._check(self._lib.fc_lbm_set_closure(self._h, None), "SetClosure")
+            return
+        keep = [np.ascontiguousarray(a, dtype=np.float32) for a in
+                (weights.w1, weights.b1, weights.w2, weights.b2, weights.w3)]
+        c = _Closure()
+        c.w1, c.b1, c.w2, c.b2, c.w3 = (a.ctypes.data_as(_FPTR) for a in keep)
+        c.b3 = float(weights.b3)
+        c.out_scale = float(weights.out_scale)
+        c.mean[:] = [float(v) for v in weights.mean]
+        c.std[:] = [float(v) for v in weights.std]
+        c.lo[:] = [float(v) for v in weights.lo]
+        c.hi[:] = [float(v) for v in weights.hi]
+        c.filter_width = float(weights.filter_width)
+        self._check(self._lib.fc_lbm_set_closure(self._h, ctypes.byref(c)), "SetClosure")
+
+    def ClosureProbe(self):
+        """(inputs (N, 4), nu_t (N,), in_range (N,) bool) of the installed
+        closure on the current populations as stored."""
+        n = self.CellCount()
+        out = np.empty(n * 5, dtype=np.float32)
+        rng = np.empty(n, dtype=np.uint8)
+        self._check(self._lib.fc_lbm_closure_probe(self._h, out.ctypes.data_as(_FP),
+                                                   rng.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), n),
+                    "ClosureProbe")
+        out = out.reshape(n, 5)
+        return out[:, :4], out[:, 4], rng.astype(bool)
+
+    def WallDistance(self) -> np.ndarray:
+        """The closure's wall-distance input, bytes in 1/16-cell steps."""
+        n = self.CellCount()
+        out = np.empty(n, dtype=np.uint8)
+        self._check(self._lib.fc_lbm_wall_distance(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), n),
+                    "WallDistance")
+        return out
 
     def ProbeSliceHealth(self, zLayer: int) -> bool:
         d = ctypes.c_int32()

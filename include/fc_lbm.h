@@ -233,6 +233,46 @@ FC_LBM_API int fc_lbm_load_populations(fc_lbm* h, const float* in, size_t count)
  * and origin from fc_lbm_init. Blocking. */
 FC_LBM_API int fc_lbm_aero_forces(fc_lbm* h, fc_aero_forces* out);
 
+/* ---- Learned sub-grid closure ----
+ * An MLP (5 inputs -> 32 -> 32 -> 1, ReLU) predicting the eddy viscosity
+ * nu_t, evaluated per cell inside the collision on the tensor cores (BF16,
+ * FP32 accumulate) in place of the constant-coefficient Smagorinsky closure
+ * (LbmReference.cpp:439-444): tau_eff = tau + 3 nu_t. This has no reference
+ * counterpart. Inputs: 0 log2(|Pi_neq|/rho), 1 tr(Pi_neq)/|Pi_neq|,
+ * 2 det(Pi_neq)/|Pi_neq|^3, 3 distance to the nearest solid cell in cells
+ * (3x3x3 chamfer, 1/16-cell steps, capped at 15.9), 4 the filter width. A
+ * cell whose inputs 0-2 leave [lo, hi] (the training range) keeps the
+ * Smagorinsky tau_eff. Weights are input-major: w1[k*32 + j] feeds input k
+ * to hidden unit j; nu_t = relu(w3 . h2 + b3) * out_scale. */
+#define FC_CLOSURE_INPUTS 5
+#define FC_CLOSURE_HIDDEN 32
+typedef struct fc_closure {
+    const float* w1; /* [5][32] */
+    const float* b1; /* [32] */
+    const float* w2; /* [32][32] */
+    const float* b2; /* [32] */
+    const float* w3; /* [32] */
+    float b3;
+    float out_scale;
+    float mean[FC_CLOSURE_INPUTS]; /* input normalization: (x - mean) / std */
+    float std[FC_CLOSURE_INPUTS];
+    float lo[3], hi[3];            /* training range of inputs 0-2 */
+    float filter_width;            /* input 4 for this lattice */
+} fc_closure;
+
+/* Installs the closure (copied; NULL returns to Smagorinsky) for every later
+ * step. Needs FP16/BF16 offset storage and an even nx
+ * (FC_LBM_ERR_UNSUPPORTED otherwise). The first call computes the wall
+ * distance field (one byte per cell). Blocking. */
+FC_LBM_API int fc_lbm_set_closure(fc_lbm* h, const fc_closure* c);
+/* The closure evaluated on the current populations as stored, by the same
+ * device code as the step: out[5*c .. 5*c+4] = inputs 0-3 and nu_t,
+ * in_range[c] = 1 where the learned nu_t is used. Host arrays; cells must be
+ * nx*ny*nz. For checking the inference. */
+FC_LBM_API int fc_lbm_closure_probe(fc_lbm* h, float* out, uint8_t* in_range, size_t cells);
+/* The wall-distance input (1/16-cell steps, 255 = 15.94 cells or more). */
+FC_LBM_API int fc_lbm_wall_distance(fc_lbm* h, uint8_t* out, size_t cells);
+
 /* Statistics of a population set computed without allocating anything: no
  * cudaMalloc, cudaFree or allocating library call happens inside. This entry
  * point has no counterpart in the reference. It is meant for callers that

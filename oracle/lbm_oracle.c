@@ -79,6 +79,11 @@ typedef struct {
     int diverged;
     real tau, inlet_u, cs;
     int reverse, slip_y, slip_z;
+    /* learned closure (see SYM(set_closure)); off when closure_on == 0 */
+    int closure_on;
+    float cw1[5 * 32], cb1[32], cw2[32 * 32], cb2[32], cw3[32], cb3;
+    float cmean[5], cinv_std[5], clo[3], chi[3], cfilter;
+    uint8_t* wall;
 } oracle_lbm;
 
 /* Lattice tables: FlowCraft/LatticeModel.h:20-43 (D3Q19) and :45-64 (D3Q15).
@@ -349,11 +354,137 @@ oracle_lbm* SYM(create)(int nx, int ny, int nz, int q, const uint8_t* solid, con
 
 void SYM(destroy)(oracle_lbm* o) {
     if (!o) return;
+    free(o->wall);
     free(o->solid);
     free(o->sdf);
     free(o->f[0]);
     free(o->f[1]);
     free(o);
+}
+
+/* ---- learned closure: the CUDA library's closure (closure.cuh) restated ----
+ * Distance to the nearest solid cell: 16 Jacobi sweeps of the 3x3x3 chamfer
+ * mask (16 / 23 / 28 sixteenths of a cell), capped at 255. */
+void SYM(wall_distance)(int nx, int ny, int nz, const uint8_t* solid, uint8_t* out) {
+    size_t n = (size_t)nx * ny * nz;
+    uint8_t* tmp = (uint8_t*)malloc(n ? n : 1);
+    for (size_t c = 0; c < n; ++c) out[c] = solid[c] ? 0 : 255;
+    for (int it = 0; it < 16; ++it) {
+        const uint8_t* in = (it % 2 == 0) ? out : tmp;
+        uint8_t* dst = (it % 2 == 0) ? tmp : out;
+        for (int z = 0; z < nz; ++z)
+            for (int y = 0; y < ny; ++y)
+                for (int x = 0; x < nx; ++x) {
+                    size_t c = ((size_t)z * ny + y) * nx + x;
+                    int best = in[c];
+                    if (best == 0) {
+                        dst[c] = 0;
+                        continue;
+                    }
+                    for (int dz = -1; dz <= 1; ++dz)
+                        for (int dy = -1; dy <= 1; ++dy)
+                            for (int dx = -1; dx <= 1; ++dx) {
+                                int xx = x + dx, yy = y + dy, zz = z + dz;
+                                int m = (dx != 0) + (dy != 0) + (dz != 0);
+                                if (m == 0 || xx < 0 || yy < 0 || zz < 0 || xx >= nx || yy >= ny || zz >= nz) continue;
+                                int cand = in[((size_t)zz * ny + yy) * nx + xx] + (m == 1 ? 16 : (m == 2 ? 23 : 28));
+                                if (cand < best) best = cand;
+                            }
+                    dst[c] = (uint8_t)(best < 255 ? best : 255);
+                }
+    }
+    free(tmp);
+}
+
+/* float -> bfloat16 -> float, round to nearest even */
+static float bf16r(float x) {
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    if ((u & 0x7fffffffu) > 0x7f800000u) return x;
+    u += 0x7fffu + ((u >> 16) & 1u);
+    u &= 0xffff0000u;
+    memcpy(&x, &u, 4);
+    return x;
+}
+
+/* Installs the closure: the weights as the library packs them (BF16 weights
+ * and hidden-layer biases, out_scale folded into the last layer, FP32 output
+ * bias), the input
+ * normalization and training range, and the wall distance (computed here
+ * when `wall` is NULL). w1 NULL turns the closure off. */
+int SYM(set_closure)(oracle_lbm* o, const float* w1, const float* b1, const float* w2, const float* b2,
+                     const float* w3, float b3, float out_scale, const float* mean, const float* std,
+                     const float* lo, const float* hi, float filter_width, const uint8_t* wall) {
+    if (!w1) {
+        o->closure_on = 0;
+        return 0;
+    }
+    for (int i = 0; i < 5 * 32; ++i) o->cw1[i] = bf16r(w1[i]);
+    for (int i = 0; i < 32 * 32; ++i) o->cw2[i] = bf16r(w2[i]);
+    for (int i = 0; i < 32; ++i) {
+        o->cb1[i] = bf16r(b1[i]);
+        o->cb2[i] = bf16r(b2[i]);
+        o->cw3[i] = bf16r(w3[i] * out_scale);
+    }
+    o->cb3 = b3 * out_scale;
+    for (int k = 0; k < 5; ++k) {
+        o->cmean[k] = mean[k];
+        o->cinv_std[k] = 1.0f / std[k];
+    }
+    for (int k = 0; k < 3; ++k) {
+        o->clo[k] = lo[k];
+        o->chi[k] = hi[k];
+    }
+    o->cfilter = filter_width;
+    if (!o->wall) o->wall = (uint8_t*)malloc(o->n ? o->n : 1);
+    if (wall)
+        memcpy(o->wall, wall, o->n);
+    else
+        SYM(wall_distance)(o->nx, o->ny, o->nz, o->solid, o->wall);
+    o->closure_on = 1;
+    return 0;
+}
+
+/* The closure's raw inputs 0-2 from Pi_neq and rho (closure_invariants). */
+static void closure_inputs(real pxx, real pyy, real pzz, real pxy, real pxz, real pyz, real rho, float* x) {
+    real pp = pxx * pxx + pyy * pyy + pzz * pzz + K(2.0) * (pxy * pxy + pxz * pxz + pyz * pyz);
+    real mag = RSQRT(pp);
+    real r = pp > K(0.0) ? K(1.0) / mag : K(0.0);
+    real inv = rho > K(1e-6) ? K(1.0) / rho : K(1.0);
+    x[0] = (float)log2((double)(mag * inv) + 1e-12);
+    x[1] = (float)((pxx + pyy + pzz) * r);
+    real det = pxx * (pyy * pzz - pyz * pyz) - pxy * (pxy * pzz - pyz * pxz) + pxz * (pxy * pyz - pyy * pxz);
+    x[2] = (float)(det * r * r * r);
+}
+
+/* nu_t of one cell, or -1 when inputs 0-2 leave the training range. Inputs,
+ * weights and hidden activations are rounded to BF16 as on the tensor cores;
+ * the sums are accumulated in double. */
+static float closure_nu(const oracle_lbm* o, const float* x3) {
+    float x[5] = {x3[0], x3[1], x3[2], x3[3], o->cfilter};
+    for (int k = 0; k < 3; ++k)
+        if (!(x[k] >= o->clo[k] && x[k] <= o->chi[k])) return -1.0f;
+    float a[5], h1[32], h2[32];
+    for (int k = 0; k < 5; ++k) a[k] = bf16r((x[k] - o->cmean[k]) * o->cinv_std[k]);
+    for (int j = 0; j < 32; ++j) {
+        double s = o->cb1[j];
+        for (int k = 0; k < 5; ++k) s += (double)a[k] * o->cw1[k * 32 + j];
+        h1[j] = bf16r(s > 0.0 ? (float)s : 0.0f);
+    }
+    for (int j = 0; j < 32; ++j) {
+        double s = o->cb2[j];
+        for (int k = 0; k < 32; ++k) s += (double)h1[k] * o->cw2[k * 32 + j];
+        h2[j] = bf16r(s > 0.0 ? (float)s : 0.0f);
+    }
+    double z = o->cb3;
+    for (int k = 0; k < 32; ++k) z += (double)h2[k] * o->cw3[k];
+    return z > 0.0 ? (float)z : 0.0f;
+}
+
+/* Batch evaluation for tests: nu_t (or -1 outside the range) of n cells from
+ * their inputs 0-3 (x[4*i .. 4*i+3]). */
+void SYM(closure_eval)(const oracle_lbm* o, const float* x, size_t n, float* nu) {
+    for (size_t i = 0; i < n; ++i) nu[i] = closure_nu(o, x + 4 * i);
 }
 
 /* ---- one fused pull-stream + BC + regularized collision step,
@@ -445,6 +576,13 @@ static void step_body(oracle_lbm* o, int z0, int z1, int tid, void* vctx) {
                 real rden = rho > K(1e-6) ? rho : K(1e-6);
                 real tau_eff = K(0.5) * (o->tau + RSQRT(o->tau * o->tau +
                                                        K(18.0) * K(1.41421356) * o->cs * o->cs * pimag / rden));
+                if (o->closure_on) { /* learned closure in place of Smagorinsky */
+                    float xin[4];
+                    closure_inputs(pxx, pyy, pzz, pxy, pxz, pyz, rho, xin);
+                    xin[3] = (float)o->wall[c] * 0.0625f;
+                    float nu = closure_nu(o, xin);
+                    if (nu >= 0.0f) tau_eff = o->tau + K(3.0) * (real)nu;
+                }
                 real omega = K(1.0) / tau_eff;
                 for (int i = 0; i < q; ++i) {
                     real ex = (real)o->ex[i], ey = (real)o->ey[i], ez = (real)o->ez[i];

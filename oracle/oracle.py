@@ -111,6 +111,11 @@ def _lib(precision: str):
         "is_ref": is_ref,
     }
     if not is_ref:
+        u8p = ctypes.POINTER(ctypes.c_uint8)
+        api["set_closure"] = fn("set_closure", c_int, vp, fptr, fptr, fptr, fptr, fptr, ctypes.c_float, ctypes.c_float,
+                                fptr, fptr, fptr, fptr, ctypes.c_float, u8p)
+        api["closure_eval"] = fn("closure_eval", None, vp, fptr, c_size, fptr)
+        api["wall_distance"] = fn("wall_distance", None, c_int, c_int, c_int, u8p, u8p)
         api["readback_field_f64"] = fn("readback_field_f64", None, vp, ctypes.POINTER(ctypes.c_double))
         api["get_populations"] = fn("get_populations", None, vp, fptr, ctypes.POINTER(ctypes.c_double))
     _loaded[precision] = api
@@ -187,6 +192,31 @@ class Oracle:
     def has_diverged(self) -> bool:
         return bool(self.api["has_diverged"](self.h))
 
+    def set_closure(self, cw, wall=None):
+        """Installs a learned closure (an object with the fields of
+        flowcraft_b200.closure.ClosureWeights), or None for Smagorinsky."""
+        fp = ctypes.POINTER(ctypes.c_float)
+        if cw is None:
+            self.api["set_closure"](self.h, None, None, None, None, None, 0.0, 0.0, None, None, None, None, 0.0, None)
+            return
+        self._closure_keep = [np.ascontiguousarray(a, dtype=np.float32) for a in
+                              (cw.w1, cw.b1, cw.w2, cw.b2, cw.w3, cw.mean, cw.std, cw.lo, cw.hi)]
+        k = [a.ctypes.data_as(fp) for a in self._closure_keep]
+        wl = None
+        if wall is not None:
+            self._wall = np.ascontiguousarray(wall, dtype=np.uint8).ravel()
+            wl = self._wall.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+        self.api["set_closure"](self.h, k[0], k[1], k[2], k[3], k[4], float(cw.b3), float(cw.out_scale), k[5], k[6],
+                                k[7], k[8], float(cw.filter_width), wl)
+
+    def closure_eval(self, inputs) -> np.ndarray:
+        """nu_t (-1 outside the training range) for rows of inputs 0-3."""
+        x = np.ascontiguousarray(inputs, dtype=np.float32).reshape(-1, 4)
+        out = np.empty(len(x), dtype=np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        self.api["closure_eval"](self.h, x.ctypes.data_as(fp), len(x), out.ctypes.data_as(fp))
+        return out
+
     def readback_field(self) -> np.ndarray:
         out = np.empty(self.n * 4, dtype=np.float32)
         self.api["readback_field"](self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
@@ -206,6 +236,16 @@ class Oracle:
         s = OracleStats()
         self.api["stats"](self.h, ctypes.byref(s))
         return s.as_dict()
+
+
+def wall_distance(solid) -> np.ndarray:
+    """The closure's wall-distance input (3x3x3 chamfer, 1/16 cells, cap 255)."""
+    solid = np.ascontiguousarray(solid, dtype=np.uint8)
+    nz, ny, nx = solid.shape
+    out = np.empty_like(solid)
+    u8p = ctypes.POINTER(ctypes.c_uint8)
+    _lib("f32")["wall_distance"](nx, ny, nz, solid.ctypes.data_as(u8p), out.ctypes.data_as(u8p))
+    return out
 
 
 # ---- voxelizer oracle (voxel_oracle.c) and the reference's Voxelizer ----
