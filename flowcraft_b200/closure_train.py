@@ -1,0 +1,272 @@
+"""Training the learned sub-grid closure on the GPU with the library's own
+kernels.
+
+Pipeline:
+  1. fine runs of the method itself (Smagorinsky, FP32 storage) on lattices
+     twice as fine as the target, sampled at several instants
+     (``LbmSolver.ClosureSamples``: 2x box filter, target eddy viscosity from
+     the sub-grid stress, inputs from the coarse cell's stress);
+  2. input normalization (mean / std) and target scaling (``out_scale``);
+  3. mini-batch Adam on the mean squared error, through
+     ``fc_lbm_mlp_grad`` / ``fc_lbm_mlp_adam`` (CUDA, deterministic);
+  4. the a-priori comparison on held-out samples against the Smagorinsky
+     closure evaluated on the same inputs, at the run's Cs and at the
+     least-squares best Cs.
+
+torch provides device buffers and the shuffling permutation only; the
+forward, backward and update arithmetic are the library's kernels.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .closure import HIDDEN, N_IN, ClosureWeights
+from .lbm import FC_LBM_OK, LbmError, load_library
+
+FC_MLP_PARAMS = 1281
+FC_MLP_GRAD_SCRATCH = 190000
+OFF = {"w1": (0, N_IN * HIDDEN), "b1": (160, HIDDEN), "w2": (192, HIDDEN * HIDDEN), "b2": (1216, HIDDEN),
+       "w3": (1248, HIDDEN), "b3": (1280, 1)}
+
+
+def _check(rc, what):
+    if rc != FC_LBM_OK:
+        raise LbmError(rc, f"{what} failed")
+
+
+def he_init(seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    p = np.zeros(FC_MLP_PARAMS, np.float32)
+    p[0:160] = rng.normal(0, math.sqrt(2.0 / N_IN), 160)
+    p[192:1216] = rng.normal(0, math.sqrt(2.0 / HIDDEN), HIDDEN * HIDDEN)
+    p[1248:1280] = rng.normal(0, math.sqrt(1.0 / HIDDEN), HIDDEN)
+    return p
+
+
+class MlpTrainer:
+    """The MLP's parameters and Adam state on one CUDA device."""
+
+    def __init__(self, params: np.ndarray, device: int = 0):
+        import torch
+        self.torch = torch
+        self.dev = torch.device("cuda", device)
+        self.lib = load_library()
+        self.p = torch.tensor(np.asarray(params, np.float32), device=self.dev)
+        self.m = torch.zeros_like(self.p)
+        self.v = torch.zeros_like(self.p)
+        self.g = torch.zeros_like(self.p)
+        self.loss = torch.zeros(1, dtype=torch.float64, device=self.dev)
+        self.scratch = torch.empty(FC_MLP_GRAD_SCRATCH, dtype=torch.float32, device=self.dev)
+        self.t = 0
+
+    def _stream(self):
+        return self.torch.cuda.current_stream(self.dev).cuda_stream
+
+    def grad(self, x, y, idx=None):
+        """(loss, grad) tensors of the mean squared error over rows idx of x, y."""
+        n = len(idx) if idx is not None else len(x)
+        _check(self.lib.fc_lbm_mlp_grad(self.p.data_ptr(), x.data_ptr(), y.data_ptr(),
+                                        idx.data_ptr() if idx is not None else None, n, self.g.data_ptr(),
+                                        self.loss.data_ptr(), self.scratch.data_ptr(), self._stream()),
+               "fc_lbm_mlp_grad")
+        return self.loss, self.g
+
+    def adam(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
+        self.t += 1
+        _check(self.lib.fc_lbm_mlp_adam(self.p.data_ptr(), self.g.data_ptr(), self.m.data_ptr(), self.v.data_ptr(),
+                                        self.t, lr, b1, b2, eps, self._stream()), "fc_lbm_mlp_adam")
+
+    def predict(self, x):
+        y = self.torch.empty(len(x), dtype=self.torch.float32, device=self.dev)
+        _check(self.lib.fc_lbm_mlp_forward(self.p.data_ptr(), x.data_ptr(), len(x), y.data_ptr(), self._stream()),
+               "fc_lbm_mlp_forward")
+        return y
+
+    def fit(self, x, y, epochs=20, batch=4096, lr=1e-3, seed=0):
+        """Mini-batch Adam; returns the mean batch loss of every epoch."""
+        torch = self.torch
+        gen = torch.Generator(device=self.dev)
+        gen.manual_seed(seed)
+        history = []
+        acc = torch.zeros(1, dtype=torch.float64, device=self.dev)
+        for _ in range(epochs):
+            perm = torch.randperm(len(x), generator=gen, device=self.dev)
+            acc.zero_()
+            nb = 0
+            for b in range(0, len(x), batch):
+                idx = perm[b:b + batch].contiguous()
+                loss, _ = self.grad(x, y, idx)
+                acc += loss
+                self.adam(lr)
+                nb += 1
+            history.append(float(acc.item()) / nb)
+        return history
+
+    def params(self) -> np.ndarray:
+        return self.p.cpu().numpy()
+
+
+@dataclass
+class TrainReport:
+    samples: int = 0
+    train_loss: list = field(default_factory=list)
+    holdout_mse: dict = field(default_factory=dict)
+    best_cs: float = 0.0
+    gain_vs_best_smagorinsky: float = 0.0
+
+
+def smagorinsky_nu(x0, tau_c: float, cs: float):
+    """The kernel's Smagorinsky eddy viscosity from input 0 (log2 |Pi|/rho):
+    tau_eff = (tau + sqrt(tau^2 + 18 sqrt2 Cs^2 |Pi|/rho)) / 2, nu = (tau_eff - tau) / 3."""
+    q = np.exp2(np.asarray(x0, np.float64))
+    te = 0.5 * (tau_c + np.sqrt(tau_c * tau_c + 18.0 * 1.41421356 * cs * cs * q))
+    return (te - tau_c) / 3.0
+
+
+def collect_samples(cases, device: int = 0, filter_width: float = 2.0):
+    """Runs each fine case and gathers closure samples at its checkpoints.
+
+    `cases`: iterable of dicts with keys solid, sdf (numpy (nz, ny, nx)), params
+    (flowcraft_b200.lbm.Params), warmup, every, count. Returns (samples tensor,
+    list of the coarse molecular tau of each case's rows)."""
+    import torch
+
+    from .lbm import LatticeModel, LbmSolver, Storage, VoxelGrid
+    chunks, taus = [], []
+    for case in cases:
+        solid = np.ascontiguousarray(case["solid"], np.uint8)
+        nz, ny, nx = solid.shape
+        s = LbmSolver()
+        g = VoxelGrid(nx, ny, nz, solid=solid.ravel(), signedDistance=case.get("sdf"))
+        if not s.Init(device, g, LatticeModel.D3Q19, Storage.FP32):
+            raise RuntimeError(s.LastError())
+        s.Reset(case["params"], True)
+        s.Step(None, case["warmup"])
+        for _ in range(case["count"]):
+            s.Step(None, case["every"])
+            rows = s.ClosureSamples(filter_width)
+            chunks.append(rows.clone())
+            taus.append(np.full(len(rows), 0.5 + 0.5 * (case["params"].tau - 0.5), np.float32))
+        s.close()
+    return torch.cat(chunks), np.concatenate(taus)
+
+
+def train_closure(samples, tau_c, device: int = 0, epochs: int = 20, batch: int = 4096, lr: float = 1e-3,
+                  seed: int = 0, holdout: float = 0.2, cs_run: float = 0.1):
+    """Trains on (1 - holdout) of the samples and compares on the rest.
+    Returns (ClosureWeights, TrainReport)."""
+    import torch
+    dev = torch.device("cuda", device)
+    samples = samples.to(dev)
+    # The eddy-viscosity fit nu* = -tau:S / (2 rho S:S) is ill-conditioned
+    # where the resolved strain is weak, and those cells put heavy tails on
+    # the targets that would dominate a squared error: keep the samples
+    # whose strain input (input 0) is above its 20th percentile and clip the
+    # targets at their 99.5th percentile.
+    x0q = torch.quantile(samples[:, 0].float()[:min(len(samples), 1 << 24)], 0.2)
+    keep = samples[:, 0] >= x0q
+    tau_c = np.asarray(tau_c)[keep.cpu().numpy()]
+    samples = samples[keep].contiguous()
+    ycap = torch.quantile(samples[:, 5][:min(len(samples), 1 << 24)], 0.995)
+    samples[:, 5] = torch.minimum(samples[:, 5], ycap)
+    n = len(samples)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed + 1)
+    perm = torch.randperm(n, generator=gen, device=dev)
+    n_tr = int(n * (1.0 - holdout))
+    tr, ho = perm[:n_tr], perm[n_tr:]
+    x, y = samples[:, :5], samples[:, 5]
+    mean = x[tr].mean(0)
+    std = x[tr].std(0).clamp_min(1e-3)
+    out_scale = float(y[tr].std().clamp_min(1e-12))
+    xn = ((x - mean) / std).contiguous()
+    yn = (y / out_scale).contiguous()
+    trainer = MlpTrainer(he_init(seed), device)
+    hist = trainer.fit(xn[tr].contiguous(), yn[tr].contiguous(), epochs, batch, lr, seed)
+    p = trainer.params()
+    cw = ClosureWeights(w1=p[0:160].reshape(N_IN, HIDDEN).copy(), b1=p[160:192].copy(),
+                        w2=p[192:1216].reshape(HIDDEN, HIDDEN).copy(), b2=p[1216:1248].copy(),
+                        w3=p[1248:1280].copy(), b3=float(p[1280]), out_scale=out_scale,
+                        mean=mean.cpu().numpy().astype(np.float32), std=std.cpu().numpy().astype(np.float32))
+    xt = x[tr][:, :3].cpu().numpy()
+    cw.lo = np.percentile(xt, 0.1, axis=0).astype(np.float32)
+    cw.hi = np.percentile(xt, 99.9, axis=0).astype(np.float32)
+    cw.filter_width = float(x[0, 4])
+    # a-priori comparison on held-out samples
+    yh = y[ho].cpu().numpy().astype(np.float64)
+    pred = np.maximum(trainer.predict(xn[ho].contiguous()).cpu().numpy().astype(np.float64), 0.0) * out_scale
+    x0h = x[ho][:, 0].cpu().numpy()
+    tch = np.asarray(tau_c)[ho.cpu().numpy()]
+    cands = np.linspace(0.0, 0.4, 401)
+    errs = [np.mean((smagorinsky_nu(x0h, tch, c) - yh) ** 2) for c in cands]
+    best = float(cands[int(np.argmin(errs))])
+    rep = TrainReport(samples=n, train_loss=hist, best_cs=best)
+    rep.holdout_mse = {"mlp": float(np.mean((pred - yh) ** 2)),
+                       "smagorinsky_run_cs": float(np.mean((smagorinsky_nu(x0h, tch, cs_run) - yh) ** 2)),
+                       "smagorinsky_best_cs": float(min(errs)), "zero": float(np.mean(yh ** 2))}
+    rep.gain_vs_best_smagorinsky = rep.holdout_mse["smagorinsky_best_cs"] / max(rep.holdout_mse["mlp"], 1e-300)
+    cw.meta = {"samples": n, "epochs": epochs, "batch": batch, "lr": lr, "seed": seed,
+               "holdout_mse": rep.holdout_mse, "best_cs": best, "train_loss": hist}
+    return cw, rep
+
+
+def c4_cases(scale: int = 1):
+    """The training set of the closure: fine lattices of 512x256x256 (divided
+    by `scale` per axis) around a sphere and a NACA 2412 wing at three
+    Reynolds numbers, Smagorinsky Cs 0.1, sampled at three instants each."""
+    from . import geometry
+    from .lbm import Params
+    nx, ny, nz = 512 // scale, 256 // scale, 256 // scale
+    u = 0.06
+    cases = []
+    sphere = geometry.sphere_grid(nx, ny, nz, nx * 0.3, ny * 0.5, nz * 0.5, nz * 0.09)
+    chord = 0.375 * nx / 2
+    wing = geometry.naca_wing_grid(nx, ny, nz, chord=chord, span=ny * 0.6, aoa_deg=6, digits="2412")
+    for (solid, sdf), lref, re in ((sphere, 2 * nz * 0.09, 5e3), (wing, chord, 2e4), (sphere, 2 * nz * 0.09, 5e4)):
+        nu = u * lref / re
+        cases.append(dict(solid=np.asarray(solid), sdf=np.asarray(sdf).ravel(),
+                          params=Params(tau=0.5 + 3 * nu, inletVelocity=u, smagorinskyCs=0.1),
+                          warmup=3 * nx, every=nx // 2, count=3))
+    return cases
+
+
+def main(argv=None):
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="train the learned closure on the GPU")
+    ap.add_argument("--scale", type=int, default=1, help="divide the 512x256x256 fine lattices by this per axis")
+    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--max-samples", type=int, default=10_000_000)
+    ap.add_argument("--out", required=True)
+    args = ap.parse_args(argv)
+    import time
+
+    import torch
+    t0 = time.time()
+    samples, tau_c = collect_samples(c4_cases(args.scale))
+    if len(samples) > args.max_samples:
+        g = torch.Generator(device=samples.device)
+        g.manual_seed(11)
+        keep = torch.randperm(len(samples), generator=g, device=samples.device)[:args.max_samples]
+        keep, _ = torch.sort(keep)
+        samples, tau_c = samples[keep], tau_c[keep.cpu().numpy()]
+    t1 = time.time()
+    cw, rep = train_closure(samples, tau_c, epochs=args.epochs, batch=args.batch, lr=args.lr)
+    t2 = time.time()
+    cw.meta.update({"fine_lattice": [512 // args.scale, 256 // args.scale, 256 // args.scale],
+                    "sample_seconds": round(t1 - t0, 1), "train_seconds": round(t2 - t1, 1),
+                    "gain_vs_best_smagorinsky": rep.gain_vs_best_smagorinsky})
+    cw.save(args.out)
+    print(json.dumps({"samples": rep.samples, "holdout_mse": rep.holdout_mse, "best_cs": rep.best_cs,
+                      "gain": rep.gain_vs_best_smagorinsky, "loss": rep.train_loss, "sample_s": t1 - t0,
+                      "train_s": t2 - t1}))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,10 +1,18 @@
-// Host-side packing of the learned closure's weights and the wall-distance
-// input (closure.cuh holds the device inference).
+// Host-side packing of the learned closure's weights, the wall-distance
+// input, and the extraction of training samples from a finer lattice
+// (closure.cuh holds the device inference).
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstring>
+#include <thread>
 
+#include <cub/device/device_scan.cuh>
+
+#include "fc_lbm.h"
+#include "lattice.cuh"
 #include "lbm_internal.h"
+#include "storage.cuh"
 
 namespace fc {
 
@@ -120,6 +128,265 @@ cudaError_t launch_wall_distance(const uint8_t* solid, const Geom& g, uint8_t* o
         e = cudaGetLastError();
     }
     return e;
+}
+
+// ---- training samples: a 2x box filter of a fine lattice ----
+//
+// Coarse cell X covers the fine cells 2X + {0,1}^3. From the fine
+// populations it gets the box-filtered density, momentum and momentum flux:
+//   rho = <rho_f>, u = <rho_f u_f> / rho,
+//   tau_sgs = <rho_f u_f u_f> - rho u u          (the sub-grid stress),
+// and, with S the strain of the filtered velocity by central differences
+// over the coarse neighbours, the target eddy viscosity is the least-squares
+// fit of tau_sgs_dev = -2 rho nu S_dev:
+//   nu* = max(0, -tau_sgs_dev : S_dev / (2 rho S_dev : S_dev)).
+// The inputs are those a coarse cell relaxing with tau_c + 3 nu* sees: the
+// regularized scheme's non-equilibrium stress is Pi = -2 rho c_s^2 tau_eff S
+// (Chapman-Enskog), so the samples carry the invariants of
+// Pi = -(2/3) rho (tau_c + 3 nu*) S, the coarse wall distance and the filter
+// width. Velocities keep their lattice value under the 2x coarsening
+// (dx and dt both double), strains and viscosities are in coarse units.
+namespace {
+
+constexpr int kCoarseFields = 10;  // rho, u (3), tau_sgs (6)
+constexpr int kWaitTimeoutMs = 600000;
+
+// Waits for `s` by polling an event with a growing sleep, so a stuck device
+// surfaces as a timeout status instead of a hang.
+cudaError_t wait_bounded(cudaStream_t s, bool* timed_out) {
+    *timed_out = false;
+    cudaEvent_t ev;
+    cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+    e = cudaEventRecord(ev, s);
+    const auto t0 = std::chrono::steady_clock::now();
+    int sleep_us = 20;
+    while (e == cudaSuccess) {
+        const cudaError_t q = cudaEventQuery(ev);
+        if (q == cudaSuccess) break;
+        if (q != cudaErrorNotReady) {
+            e = q;
+            break;
+        }
+        if (std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(kWaitTimeoutMs)) {
+            *timed_out = true;
+            break;
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(sleep_us));
+        if (sleep_us < 2000) sleep_us *= 2;
+    }
+    cudaEventDestroy(ev);
+    return e;
+}
+
+template <int Q, class S>
+__global__ void k_coarse_fields(const typename S::T* __restrict__ f, const uint8_t* __restrict__ solid, Geom fg,
+                                Geom cg, uint8_t* __restrict__ csolid, float* __restrict__ cf) {
+    using L = Lattice<Q>;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < cg.n; c += (size_t)gridDim.x * blockDim.x) {
+        const int zc = (int)(c / (size_t)cg.nxy);
+        const size_t rem = c - (size_t)zc * cg.nxy;
+        const int yc = (int)(rem / cg.nx);
+        const int xc = (int)(rem - (size_t)yc * cg.nx);
+        bool any_solid = false;
+        double rs = 0, mx = 0, my = 0, mz = 0, uu[6] = {0, 0, 0, 0, 0, 0};
+        for (int k = 0; k < 8; ++k) {
+            const size_t fc = ((size_t)(2 * zc + (k >> 2)) * fg.ny + (2 * yc + ((k >> 1) & 1))) * fg.nx +
+                              (2 * xc + (k & 1));
+            if (solid[fc]) {
+                any_solid = true;
+                continue;
+            }
+            float rho = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
+            static_for<0, Q>([&](auto I) {
+                constexpr int i = decltype(I)::value;
+                const float v = load_pop_c<Q, S, i>(f, fg.n, fc);
+                rho += v;
+                if constexpr (L::ex(i) != 0) jx += (float)L::ex(i) * v;
+                if constexpr (L::ey(i) != 0) jy += (float)L::ey(i) * v;
+                if constexpr (L::ez(i) != 0) jz += (float)L::ez(i) * v;
+            });
+            const double ux = jx / rho, uy = jy / rho, uz = jz / rho;
+            rs += rho;
+            mx += jx, my += jy, mz += jz;
+            uu[0] += rho * ux * ux, uu[1] += rho * uy * uy, uu[2] += rho * uz * uz;
+            uu[3] += rho * ux * uy, uu[4] += rho * ux * uz, uu[5] += rho * uy * uz;
+        }
+        csolid[c] = any_solid ? 1 : 0;
+        float* o = cf + c * kCoarseFields;
+        if (any_solid) {
+            for (int k = 0; k < kCoarseFields; ++k) o[k] = 0.0f;
+            continue;
+        }
+        const double rho = rs / 8.0, ux = mx / rs, uy = my / rs, uz = mz / rs;
+        o[0] = (float)rho, o[1] = (float)ux, o[2] = (float)uy, o[3] = (float)uz;
+        o[4] = (float)(uu[0] / 8.0 - rho * ux * ux), o[5] = (float)(uu[1] / 8.0 - rho * uy * uy);
+        o[6] = (float)(uu[2] / 8.0 - rho * uz * uz), o[7] = (float)(uu[3] / 8.0 - rho * ux * uy);
+        o[8] = (float)(uu[4] / 8.0 - rho * ux * uz), o[9] = (float)(uu[5] / 8.0 - rho * uy * uz);
+    }
+}
+
+struct SampleOut {
+    bool valid;
+    float row[6];
+};
+
+__device__ SampleOut coarse_sample(const uint8_t* __restrict__ csolid, const float* __restrict__ cf,
+                                   const uint8_t* __restrict__ cwall, const Geom& cg, size_t c, float tau_c,
+                                   float filter_width) {
+    SampleOut r{};
+    const int z = (int)(c / (size_t)cg.nxy);
+    const size_t rem = c - (size_t)z * cg.nxy;
+    const int y = (int)(rem / cg.nx);
+    const int x = (int)(rem - (size_t)y * cg.nx);
+    // off the inlet/outlet planes and the domain faces, with fluid neighbours
+    if (x < 2 || x > cg.nx - 3 || y < 1 || y > cg.ny - 2 || z < 1 || z > cg.nz - 2 || csolid[c]) return r;
+    const size_t nb[6] = {c - 1, c + 1, c - (size_t)cg.nx, c + (size_t)cg.nx, c - (size_t)cg.nxy, c + (size_t)cg.nxy};
+    for (int k = 0; k < 6; ++k)
+        if (csolid[nb[k]]) return r;
+    double g[3][3];  // g[a][b] = d u_b / d x_a
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) g[a][b] = 0.5 * ((double)cf[nb[2 * a + 1] * kCoarseFields + 1 + b] -
+                                                       (double)cf[nb[2 * a] * kCoarseFields + 1 + b]);
+    double sm[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) sm[a][b] = 0.5 * (g[a][b] + g[b][a]);
+    const double tr = (sm[0][0] + sm[1][1] + sm[2][2]) / 3.0;
+    double sd[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) sd[a][b] = sm[a][b] - (a == b ? tr : 0.0);
+    const float* o = cf + c * kCoarseFields;
+    const double rho = o[0];
+    const double t6[6] = {o[4], o[5], o[6], o[7], o[8], o[9]};
+    const double ttr = (t6[0] + t6[1] + t6[2]) / 3.0;
+    const double td[3][3] = {{t6[0] - ttr, t6[3], t6[4]}, {t6[3], t6[1] - ttr, t6[5]}, {t6[4], t6[5], t6[2] - ttr}};
+    double tds = 0.0, sds = 0.0;
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            tds += td[a][b] * sd[a][b];
+            sds += sd[a][b] * sd[a][b];
+        }
+    if (!(sds > 1e-18) || !(rho > 0.0)) return r;
+    double nu = -tds / (2.0 * rho * sds);
+    nu = nu > 0.0 ? nu : 0.0;
+    // the stress a coarse cell relaxing with tau_c + 3 nu carries
+    const double k = -(2.0 / 3.0) * rho * ((double)tau_c + 3.0 * nu);
+    double p[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) p[a][b] = k * sm[a][b];
+    double pp = 0.0;
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) pp += p[a][b] * p[a][b];
+    const double mag = sqrt(pp);
+    const double ri = mag > 0.0 ? 1.0 / mag : 0.0;
+    const double det = p[0][0] * (p[1][1] * p[2][2] - p[1][2] * p[2][1]) -
+                       p[0][1] * (p[1][0] * p[2][2] - p[1][2] * p[2][0]) +
+                       p[0][2] * (p[1][0] * p[2][1] - p[1][1] * p[2][0]);
+    r.row[0] = (float)log2(mag / rho + 1e-12);
+    r.row[1] = (float)((p[0][0] + p[1][1] + p[2][2]) * ri);
+    r.row[2] = (float)(det * ri * ri * ri);
+    r.row[3] = (float)cwall[c] * 0.0625f;
+    r.row[4] = filter_width;
+    r.row[5] = (float)nu;
+    r.valid = true;
+    return r;
+}
+
+__global__ void k_sample_flags(const uint8_t* __restrict__ csolid, const float* __restrict__ cf,
+                               const uint8_t* __restrict__ cwall, Geom cg, float tau_c, float filter_width,
+                               uint32_t* __restrict__ flags) {
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < cg.n; c += (size_t)gridDim.x * blockDim.x)
+        flags[c] = coarse_sample(csolid, cf, cwall, cg, c, tau_c, filter_width).valid ? 1u : 0u;
+}
+
+__global__ void k_sample_write(const uint8_t* __restrict__ csolid, const float* __restrict__ cf,
+                               const uint8_t* __restrict__ cwall, Geom cg, float tau_c, float filter_width,
+                               const uint32_t* __restrict__ pos, float* __restrict__ out) {
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < cg.n; c += (size_t)gridDim.x * blockDim.x) {
+        const SampleOut so = coarse_sample(csolid, cf, cwall, cg, c, tau_c, filter_width);
+        if (!so.valid) continue;
+        float* row = out + (size_t)pos[c] * 6;
+        for (int k = 0; k < 6; ++k) row[k] = so.row[k];
+    }
+}
+
+template <int Q, class S>
+cudaError_t coarse_fields_t(const void* f, const uint8_t* solid, const Geom& fg, const Geom& cg, uint8_t* csolid,
+                            float* cf, cudaStream_t s) {
+    const int blocks = (int)((cg.n + 255) / 256 < 148 * 16 ? (cg.n + 255) / 256 : 148 * 16);
+    k_coarse_fields<Q, S><<<blocks, 256, 0, s>>>((const typename S::T*)f, solid, fg, cg, csolid, cf);
+    return cudaGetLastError();
+}
+
+cudaError_t coarse_fields(int q, int storage, const void* f, const uint8_t* solid, const Geom& fg, const Geom& cg,
+                          uint8_t* csolid, float* cf, cudaStream_t s) {
+    if (q == 19) {
+        if (storage == 0) return coarse_fields_t<19, StoreF32>(f, solid, fg, cg, csolid, cf, s);
+        if (storage == 1) return coarse_fields_t<19, StoreF16>(f, solid, fg, cg, csolid, cf, s);
+        if (storage == 2) return coarse_fields_t<19, StoreBF16>(f, solid, fg, cg, csolid, cf, s);
+    } else if (q == 15) {
+        if (storage == 0) return coarse_fields_t<15, StoreF32>(f, solid, fg, cg, csolid, cf, s);
+        if (storage == 1) return coarse_fields_t<15, StoreF16>(f, solid, fg, cg, csolid, cf, s);
+        if (storage == 2) return coarse_fields_t<15, StoreBF16>(f, solid, fg, cg, csolid, cf, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace
+
+int closure_samples(int q, int storage, const void* f, const uint8_t* solid, const Geom& fg, float tau_c,
+                    float filter_width, float* out, int64_t capacity, int64_t* count, cudaStream_t s) {
+    Geom cg{};
+    cg.nx = fg.nx / 2, cg.ny = fg.ny / 2, cg.nz = fg.nz / 2;
+    cg.wpr = (cg.nx + 31) / 32;
+    cg.nxy = (long long)cg.nx * cg.ny;
+    cg.n = (size_t)cg.nx * cg.ny * cg.nz;
+    *count = 0;
+    if (cg.nx < 5 || cg.ny < 3 || cg.nz < 3) return FC_LBM_ERR_INVALID_ARG;
+    uint8_t *csolid = nullptr, *cwall = nullptr, *tmp = nullptr;
+    float* cf = nullptr;
+    uint32_t *flags = nullptr, *pos = nullptr;
+    void* scan_tmp = nullptr;
+    size_t scan_bytes = 0;
+    int rc = FC_LBM_OK;
+    auto ok = [&](cudaError_t e) {
+        if (e != cudaSuccess && rc == FC_LBM_OK) rc = e == cudaErrorMemoryAllocation ? FC_LBM_ERR_OUT_OF_MEMORY
+                                                                                     : FC_LBM_ERR_CUDA;
+        return rc == FC_LBM_OK;
+    };
+    const int blocks = (int)((cg.n + 255) / 256 < 148 * 16 ? (cg.n + 255) / 256 : 148 * 16);
+    uint32_t total = 0;
+    bool timed_out = false;
+    if (ok(cudaMallocAsync(&csolid, cg.n, s)) && ok(cudaMallocAsync(&cwall, cg.n, s)) &&
+        ok(cudaMallocAsync(&tmp, cg.n, s)) && ok(cudaMallocAsync(&cf, cg.n * kCoarseFields * sizeof(float), s)) &&
+        ok(cudaMallocAsync(&flags, cg.n * sizeof(uint32_t), s)) &&
+        ok(cudaMallocAsync(&pos, (cg.n + 1) * sizeof(uint32_t), s)) &&
+        ok(coarse_fields(q, storage, f, solid, fg, cg, csolid, cf, s)) &&
+        ok(launch_wall_distance(csolid, cg, cwall, tmp, s))) {
+        k_sample_flags<<<blocks, 256, 0, s>>>(csolid, cf, cwall, cg, tau_c, filter_width, flags);
+        if (ok(cudaGetLastError()) && ok(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, flags, pos, (int64_t)cg.n, s)) &&
+            ok(cudaMallocAsync(&scan_tmp, scan_bytes, s)) &&
+            ok(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, flags, pos, (int64_t)cg.n, s))) {
+            uint32_t last[2] = {0, 0};
+            if (ok(cudaMemcpyAsync(&last[0], pos + cg.n - 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s)) &&
+                ok(cudaMemcpyAsync(&last[1], flags + cg.n - 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s)) &&
+                ok(wait_bounded(s, &timed_out))) {
+                if (timed_out) rc = FC_LBM_ERR_TIMEOUT;
+                total = last[0] + last[1];
+                *count = total;
+                if (rc != FC_LBM_OK) {
+                } else if ((int64_t)total > capacity) {
+                    rc = FC_LBM_ERR_TOO_LARGE;
+                } else if (out && total > 0) {
+                    k_sample_write<<<blocks, 256, 0, s>>>(csolid, cf, cwall, cg, tau_c, filter_width, pos, out);
+                    ok(cudaGetLastError());
+                }
+            }
+        }
+    }
+    for (void* p : {(void*)csolid, (void*)cwall, (void*)tmp, (void*)cf, (void*)flags, (void*)pos, scan_tmp})
+        if (p) cudaFreeAsync(p, s);
+    return rc;
 }
 
 }  // namespace fc

@@ -749,6 +749,20 @@ int fc_lbm_set_closure(fc_lbm* h, const fc_closure* c) {
     return FC_LBM_OK;
 }
 
+int fc_lbm_closure_samples(fc_lbm* h, float filter_width, float* out, int64_t capacity, int64_t* count) {
+    FC_RC(check_ready(h));
+    if (!count || capacity < 0 || !std::isfinite(filter_width)) return FC_LBM_ERR_INVALID_ARG;
+    DeviceGuard dg(h->device);
+    FC_RC(wait_stream(h, kTransferTimeoutMs));  // every queued step first
+    // the molecular relaxation time of the 2x coarser lattice (nu halves)
+    const float tau_c = 0.5f + 0.5f * (h->params.tau - 0.5f);
+    const int rc = fc::closure_samples(h->q, h->storage, h->pop[h->cur], h->d_solid, h->g, tau_c, filter_width, out,
+                                       capacity, count, h->stream);
+    h->launches += 5;
+    if (rc != FC_LBM_OK && rc != FC_LBM_ERR_TOO_LARGE) return fail(h, rc, "closure samples failed");
+    return rc;
+}
+
 int fc_lbm_closure_probe(fc_lbm* h, float* out, uint8_t* in_range, size_t cells) {
     FC_RC(check_ready(h));
     if (!h->closure_on) return fail(h, FC_LBM_ERR_NOT_INITIALIZED, "no learned closure set");

@@ -107,6 +107,14 @@ void pack_closure(const float* w1, const float* b1, const float* w2, const float
 // nearest solid cell; `tmp` is a scratch array of g.n bytes.
 cudaError_t launch_wall_distance(const uint8_t* solid, const Geom& g, uint8_t* out, uint8_t* tmp, cudaStream_t s);
 
+// Training samples of the closure from a 2x box filter of this lattice
+// (closure.cu): rows (inputs 0-4, target nu_t) written to device `out` in
+// coarse cell order. Returns an FC_LBM_* status; *count is the sample count
+// (also when it exceeds `capacity`, FC_LBM_ERR_TOO_LARGE). Waits for `s`
+// (bounded: FC_LBM_ERR_TIMEOUT).
+int closure_samples(int q, int storage, const void* f, const uint8_t* solid, const Geom& fg, float tau_c,
+                    float filter_width, float* out, int64_t capacity, int64_t* count, cudaStream_t s);
+
 cudaError_t launch_bulk_pull_learned(int q, int storage, const void* fin, void* fout, const uint32_t* bulk_bits,
                                      const Geom& g, const StepParams& p, int z0, int zc, int* diverged,
                                      cudaStream_t s, int* launched, const ClosureDev& cl);

@@ -149,6 +149,11 @@ SIGNATURES = {
     "fc_lbm_set_closure": (ctypes.c_int, [_P, ctypes.POINTER(_Closure)]),
     "fc_lbm_closure_probe": (ctypes.c_int, [_P, _FP, ctypes.POINTER(ctypes.c_uint8), _SZ]),
     "fc_lbm_wall_distance": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint8), _SZ]),
+    "fc_lbm_closure_samples": (ctypes.c_int, [_P, ctypes.c_float, _P, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
+    "fc_lbm_mlp_forward": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P, _P]),
+    "fc_lbm_mlp_grad": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int64, _P, _P, _P, _P]),
+    "fc_lbm_mlp_adam": (ctypes.c_int, [_P, _P, _P, _P, _I32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                       ctypes.c_float, _P]),
     "fc_lbm_voxel_grid": (ctypes.c_int, [_P, _SZ, ctypes.POINTER(_VoxelParams), _I32, _I32P, _FP, _FP, _P]),
     "fc_lbm_voxelize": (ctypes.c_int, [_P, _SZ, _P, _SZ, _I32P, ctypes.c_float, _FP, _I32, _P, _P, _P]),
 }
@@ -273,6 +278,7 @@ class LbmSolver:
         self._h = h
         self._solid_cpu = np.zeros(0, dtype=np.uint8)
         self._model = LatticeModel.D3Q19
+        self._device = 0
         self._keep = []
 
     # -- lifetime --------------------------------------------------------
@@ -300,6 +306,7 @@ class LbmSolver:
     def Init(self, device, grid: VoxelGrid, model: LatticeModel = LatticeModel.D3Q19,
              storage: Storage = Storage.FP32, streaming: Streaming = Streaming.PINGPONG) -> bool:
         """LbmSolver::Init (LbmSolver.cpp:205-366); ``device`` is a CUDA ordinal."""
+        self._device = int(device)
         desc = _GridDesc()
         desc.nx, desc.ny, desc.nz = grid.nx, grid.ny, grid.nz
         desc.cell_size = grid.cellSize
@@ -437,6 +444,22 @@ class LbmSolver:
                     "ClosureProbe")
         out = out.reshape(n, 5)
         return out[:, :4], out[:, 4], rng.astype(bool)
+
+    def ClosureSamples(self, filterWidth: float = 2.0, out=None):
+        """Training samples of the closure from a 2x box filter of this
+        lattice: a CUDA tensor (rows, 6) of inputs 0-4 and the target nu_t
+        (allocated here when `out` is None)."""
+        import torch
+        cnt = ctypes.c_int64(0)
+        rc = self._lib.fc_lbm_closure_samples(self._h, float(filterWidth), None, 0, ctypes.byref(cnt))
+        if rc not in (FC_LBM_OK, FC_LBM_ERR_TOO_LARGE):
+            self._check(rc, "ClosureSamples")
+        n = int(cnt.value)
+        if out is None:
+            out = torch.empty((max(n, 1), 6), dtype=torch.float32, device=f"cuda:{self._device}")
+        self._check(self._lib.fc_lbm_closure_samples(self._h, float(filterWidth), out.data_ptr(), out.shape[0],
+                                                     ctypes.byref(cnt)), "ClosureSamples")
+        return out[:n]
 
     def WallDistance(self) -> np.ndarray:
         """The closure's wall-distance input, bytes in 1/16-cell steps."""

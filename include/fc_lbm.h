@@ -273,6 +273,37 @@ FC_LBM_API int fc_lbm_closure_probe(fc_lbm* h, float* out, uint8_t* in_range, si
 /* The wall-distance input (1/16-cell steps, 255 = 15.94 cells or more). */
 FC_LBM_API int fc_lbm_wall_distance(fc_lbm* h, uint8_t* out, size_t cells);
 
+/* Training samples for the closure from this (fine) lattice: its current
+ * populations are box-filtered 2x2x2 onto a lattice of half the size; every
+ * coarse cell off the faces and the inlet/outlet planes whose 6 neighbours
+ * are fluid gives one row of 6 floats (inputs 0-4 and the target nu_t),
+ * written to the DEVICE array `out` in coarse-cell order. The target is the
+ * least-squares eddy viscosity of the sub-grid stress of the filtered flow
+ * against its resolved strain (central differences); the inputs are those
+ * of a coarse cell relaxing with the coarse molecular tau plus 3 nu_t.
+ * *count receives the number of rows; with out NULL or capacity too small
+ * nothing is written (FC_LBM_ERR_TOO_LARGE when rows did not fit). Blocking.
+ * No reference counterpart. */
+FC_LBM_API int fc_lbm_closure_samples(fc_lbm* h, float filter_width, float* out, int64_t capacity, int64_t* count);
+
+/* ---- Training the closure's MLP (no reference counterpart) ----
+ * params: FC_MLP_PARAMS floats, w1[5*32], b1[32], w2[32*32], b2[32], w3[32],
+ * b3 (the fc_closure layout, unscaled), on the device like every array here.
+ * x: n rows of the 5 normalized inputs; y: n targets. The output is linear
+ * (training); inference applies relu and out_scale. All calls are
+ * asynchronous on `stream`. */
+#define FC_MLP_PARAMS 1281
+#define FC_MLP_GRAD_SCRATCH 190000 /* floats */
+FC_LBM_API int fc_lbm_mlp_forward(const float* params, const float* x, int64_t n, float* y, void* stream);
+/* grad = d/dparams of the mean squared error over rows idx[0..n) (idx NULL:
+ * rows 0..n-1), *loss (device double, or NULL) = that error. Deterministic:
+ * the same inputs give the same bits. scratch: FC_MLP_GRAD_SCRATCH floats. */
+FC_LBM_API int fc_lbm_mlp_grad(const float* params, const float* x, const float* y, const int64_t* idx, int64_t n,
+                               float* grad, double* loss, float* scratch, void* stream);
+/* One Adam step (Kingma & Ba 2015) with bias correction; step counts from 1. */
+FC_LBM_API int fc_lbm_mlp_adam(float* params, const float* grad, float* m, float* v, int32_t step, float lr,
+                               float beta1, float beta2, float eps, void* stream);
+
 /* Statistics of a population set computed without allocating anything: no
  * cudaMalloc, cudaFree or allocating library call happens inside. This entry
  * point has no counterpart in the reference. It is meant for callers that
