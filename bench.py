@@ -11,8 +11,12 @@ analytically on the device; there is no mesh file or dataset.
 One "step" is one full lattice update (every cell streamed, collided and
 written). ``value`` = whole-job GLUPS (cells x steps / s, solid cells
 included) with the lattice resident in HBM, timed with CUDA events on the
-solver's stream, max over ranks. The headline storage is FP16 offset
-populations with FP32 collision; the plain FP32 path is timed beside it.
+solver's stream, max over ranks. The headline is the metric's pairing: FP16
+offset populations with the learned sub-grid closure (the MLP trained by
+flowcraft_b200.closure_train, flowcraft_b200/data/closure_c4.json, evaluated
+per cell on the tensor cores inside the collision); FP16 with plain
+Smagorinsky and the plain FP32 path (bit-identical to the reference) are
+timed beside it.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 For N > 1 run under torchrun; every rank steps its own lattice (replicas, no
@@ -50,7 +54,10 @@ CONFIGS = {
                     "Re=1e4 (tau=0.50173), Smagorinsky Cs=0.1"),
 }
 
-BYTES_PER_ELEM = {"fp32": 4, "fp16_offset": 2, "bf16_offset": 2}
+BYTES_PER_ELEM = {"fp32": 4, "fp16_offset": 2, "bf16_offset": 2, "fp16_learned": 2, "bf16_learned": 2}
+# per-cell bytes beyond the populations: the closure's wall-distance byte
+EXTRA_BYTES = {"fp16_learned": 1, "bf16_learned": 1}
+CLOSURE_WEIGHTS = os.path.join(ROOT, "flowcraft_b200", "data", "closure_c4.json")
 
 
 def parse_args(argv=None):
@@ -60,7 +67,7 @@ def parse_args(argv=None):
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="large")
-    ap.add_argument("--variants", default="fp16_offset,fp32", help="first one is the headline")
+    ap.add_argument("--variants", default="fp16_learned,fp16_offset,fp32", help="first one is the headline")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -137,14 +144,14 @@ def measured_peak():
 
 
 def ncu_traffic_per_cell(variant: str):
-    """DRAM bytes per bulk-kernel cell update from the committed ncu summary
-    (a line 'traffic_bytes_per_cell <kernel> <variant> = X'), or None."""
-    path = os.path.join(ROOT, "profiles", "bulk_pull_ncu.md")
+    """DRAM bytes per bulk cell update from the committed ncu summary of the
+    bulk kernels (a line 'traffic_bytes_per_cell <variant> = X'), or None."""
+    path = os.path.join(ROOT, "profiles", "bulk_pairs_ncu_c2.md")
     try:
         text = open(path).read()
     except OSError:
         return None
-    m = re.search(rf"traffic_bytes_per_cell\s+bulk_pull\s+{variant}\s*=\s*([0-9.]+)", text)
+    m = re.search(rf"traffic_bytes_per_cell\s+{variant}\s*=\s*([0-9.]+)", text)
     return float(m.group(1)) if m else None
 
 
@@ -165,14 +172,22 @@ def build_geometry(cfg, device, z_lo=0, z_hi=None):
     return solid[z_lo:z_hi].contiguous(), sdf[z_lo:z_hi].contiguous()
 
 
+def storage_of(variant):
+    from flowcraft_b200 import Storage
+    return {"fp32": Storage.FP32, "fp16_offset": Storage.FP16_OFFSET, "bf16_offset": Storage.BF16_OFFSET,
+            "fp16_learned": Storage.FP16_OFFSET, "bf16_learned": Storage.BF16_OFFSET}[variant]
+
+
 def make_solver(cfg, solid, sdf, variant, device_index):
-    from flowcraft_b200 import LatticeModel, LbmSolver, Params, Storage, VoxelGrid
+    from flowcraft_b200 import LatticeModel, LbmSolver, Params, VoxelGrid
     s = LbmSolver()
-    st = {"fp32": Storage.FP32, "fp16_offset": Storage.FP16_OFFSET, "bf16_offset": Storage.BF16_OFFSET}[variant]
     grid = VoxelGrid(cfg["nx"], cfg["ny"], cfg["nz"], solid=solid, signedDistance=sdf)
-    if not s.Init(device_index, grid, LatticeModel.D3Q19, st):
+    if not s.Init(device_index, grid, LatticeModel.D3Q19, storage_of(variant)):
         raise RuntimeError(s.LastError())
     s.Reset(Params(tau=tau_for(cfg), inletVelocity=cfg["u"], smagorinskyCs=cfg["cs"]), True)
+    if variant.endswith("_learned"):
+        from flowcraft_b200.closure import ClosureWeights
+        s.SetClosure(ClosureWeights.load(CLOSURE_WEIGHTS))
     return s
 
 
@@ -280,7 +295,8 @@ def time_variant(args, cfg, solid, sdf, variant, dev_index, dist_on, sample_cloc
     cells = cfg["nx"] * cfg["ny"] * cfg["nz"]
     elem = BYTES_PER_ELEM[variant]
     bulk_avg_s = t["bulk_ms"] / args.steps / 1e3
-    bulk_bytes = info["bulk_cells"] * 19 * 2 * elem
+    per_cell = 19 * 2 * elem + EXTRA_BYTES.get(variant, 0)
+    bulk_bytes = info["bulk_cells"] * per_cell
     return {
         "variant": variant, "total_ms": total_ms, "ms_per_step": total_ms / args.steps,
         "glups_rank": cells * args.steps / (t["total_ms"] / 1e3) / 1e9,
@@ -288,7 +304,7 @@ def time_variant(args, cfg, solid, sdf, variant, dev_index, dist_on, sample_cloc
         "bulk_cells": info["bulk_cells"], "boundary_cells": info["boundary_cells"],
         "bouzidi_links": info["bouzidi_links"], "bulk_bytes_per_launch": bulk_bytes,
         "bulk_gbs": bulk_bytes / bulk_avg_s / 1e9 if bulk_avg_s > 0 else None,
-        "launches": launches, "clocks": clocks, "bytes_per_cell": 19 * 2 * elem,
+        "launches": launches, "clocks": clocks, "bytes_per_cell": per_cell,
         "stats_after": {"avg_density": stats.avgDensity, "avg_speed": stats.avgSpeed, "has_nan": stats.hasNaN,
                         "force_x": stats.forceX, "force_z": stats.forceZ},
     }
@@ -309,7 +325,7 @@ def run_e2e(args, cfg, solid, sdf, variant, dev_index):
     out = np.empty(n * 4, dtype=np.float32)
     out[::1024] = 0  # fault the pages in before timing
     out.fill(0)
-    st = {"fp32": Storage.FP32, "fp16_offset": Storage.FP16_OFFSET, "bf16_offset": Storage.BF16_OFFSET}[variant]
+    st = storage_of(variant)
     grid = VoxelGrid(cfg["nx"], cfg["ny"], cfg["nz"], solid=h_solid.numpy(), signedDistance=h_sdf.numpy())
     torch.cuda.synchronize()
     s = LbmSolver()
@@ -317,6 +333,9 @@ def run_e2e(args, cfg, solid, sdf, variant, dev_index):
     if not s.Init(dev_index, grid, LatticeModel.D3Q19, st):
         raise RuntimeError(s.LastError())
     s.Reset(Params(tau=tau_for(cfg), inletVelocity=cfg["u"], smagorinskyCs=cfg["cs"]), True)
+    if variant.endswith("_learned"):
+        from flowcraft_b200.closure import ClosureWeights
+        s.SetClosure(ClosureWeights.load(CLOSURE_WEIGHTS))
     diverged = False
     for k in range(args.steps):
         s.Step(None, 1)
@@ -331,8 +350,8 @@ def run_e2e(args, cfg, solid, sdf, variant, dev_index):
     return {"value": n * args.steps / el / 1e9, "unit": "GLUPS", "seconds": el,
             "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
             "diverged": diverged, "avg_density": stats.avgDensity,
-            "timed": "Init(host VoxelGrid) + Reset + steps x (Step(1) + ProbeSliceHealth) + ReadbackStats + "
-                     "ReadbackFieldRange(all z)"}
+            "timed": "Init(host VoxelGrid) + Reset + SetClosure (learned variants) + steps x (Step(1) + "
+                     "ProbeSliceHealth) + ReadbackStats + ReadbackFieldRange(all z)"}
 
 
 def run_ours(args, cfg, rank, world, local_rank):
@@ -358,7 +377,8 @@ def run_ours(args, cfg, rank, world, local_rank):
         "bound": "hbm", "achieved": head["bulk_gbs"], "peak": peak, "unit": "GB/s",
         "frac": head["bulk_gbs"] / peak if head["bulk_gbs"] else None,
         "traffic": trf * head["bulk_cells"] if trf else None,
-        "kernel": f"k_bulk_interior<19,{head['variant']}> + k_bulk_shell (all bulk-mask cells)",
+        "kernel": (f"k_bulk_pairs_learned<19,{head['variant']}>" if head["variant"].endswith("_learned")
+                   else f"k_bulk_pairs<19,{head['variant']}>") + " (all bulk-mask cells)",
         "algorithmic_bytes_per_launch": head["bulk_bytes_per_launch"],
         "peak_source": f"{peak_src} ({'MEASURED_PEAKS.json hbm_gbs' if peak_src == 'measured' else 'fallback'})",
     }
@@ -390,8 +410,11 @@ def run_ours(args, cfg, rank, world, local_rank):
         "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: analytic procedural geometry built on the device, no dataset",
         "config": {"workload": cfg["desc"], "lattice": "D3Q19", "nx": cfg["nx"], "ny": cfg["ny"], "nz": cfg["nz"],
-                   "cells": cells, "storage": head["variant"], "collision": "regularized + Smagorinsky, FP32",
-                   "closure": "Smagorinsky (learned closure not built yet)", "streaming": "pull, ping-pong",
+                   "cells": cells, "storage": head["variant"], "collision": "regularized, FP32",
+                   "closure": ("learned MLP 5-32-32-1 (BF16 tensor-core MMA, FP32 accumulate) per cell, Smagorinsky "
+                               "Cs=0.1 outside its training range; weights flowcraft_b200/data/closure_c4.json"
+                               if head["variant"].endswith("_learned") else "Smagorinsky"),
+                   "streaming": "pull, ping-pong",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "no flush: the population set (10.2 GB fp16 / 20.4 GB fp32 per copy) exceeds the 126 MB L2",
                    "boundary_cells": head["boundary_cells"], "bouzidi_links": head["bouzidi_links"]},

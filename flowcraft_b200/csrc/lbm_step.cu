@@ -457,8 +457,12 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned(const 
     closure_invariants(mo.pxx.x, mo.pyy.x, mo.pzz.x, mo.pxy.x, mo.pxz.x, mo.pyz.x, mo.pp.x, mo.inv.x, xa0, xa1, xa2);
     closure_invariants(mo.pxx.y, mo.pyy.y, mo.pzz.y, mo.pxy.y, mo.pxz.y, mo.pyz.y, mo.pp.y, mo.inv.y, xb0, xb1, xb2);
     const bool la = closure_in_range(cl, xa0, xa1, xa2), lb = closure_in_range(cl, xb0, xb1, xb2);
-    const float sga = smagorinsky_g(mo.pp.x, mo.rho.x, mo.inv.x, p.tau, p.cs);
-    const float sgb = smagorinsky_g(mo.pp.y, mo.rho.y, mo.inv.y, p.tau, p.cs);
+    // the Smagorinsky fallback only where some lane of the warp needs it
+    float sga = 0.0f, sgb = 0.0f;
+    if (__any_sync(0xffffffffu, !(la && lb))) {
+        sga = smagorinsky_g(mo.pp.x, mo.rho.x, mo.inv.x, p.tau, p.cs);
+        sgb = smagorinsky_g(mo.pp.y, mo.rho.y, mo.inv.y, p.tau, p.cs);
+    }
     uint32_t* in = &s_in[threadIdx.y][threadIdx.x * 8];
     closure_pack_inputs(cl, xa0, xa1, xa2, (float)(wd & 0xffu) * 0.0625f, in);
     closure_pack_inputs(cl, xb0, xb1, xb2, (float)(wd >> 8) * 0.0625f, in + 4);
