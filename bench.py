@@ -287,6 +287,7 @@ def time_variant(args, cfg, solid, sdf, variant, dev_index, dist_on, sample_cloc
     l0 = s.LaunchCount()
     t = s.StepTimed(args.steps)  # events around every launch, waits at the end
     launches = s.LaunchCount() - l0
+    coverage = s.ClosureCoverage() if variant.endswith("_learned") else None
     clocks = sampler.stop() if sampler else None
     barrier_sync(dist_on)
     total_ms = allreduce_max(t["total_ms"], dist_on)
@@ -304,7 +305,7 @@ def time_variant(args, cfg, solid, sdf, variant, dev_index, dist_on, sample_cloc
         "bulk_cells": info["bulk_cells"], "boundary_cells": info["boundary_cells"],
         "bouzidi_links": info["bouzidi_links"], "bulk_bytes_per_launch": bulk_bytes,
         "bulk_gbs": bulk_bytes / bulk_avg_s / 1e9 if bulk_avg_s > 0 else None,
-        "launches": launches, "clocks": clocks, "bytes_per_cell": per_cell,
+        "launches": launches, "clocks": clocks, "bytes_per_cell": per_cell, "closure_coverage": coverage,
         "stats_after": {"avg_density": stats.avgDensity, "avg_speed": stats.avgSpeed, "has_nan": stats.hasNaN,
                         "force_x": stats.forceX, "force_z": stats.forceZ},
     }
@@ -403,6 +404,7 @@ def run_ours(args, cfg, rank, world, local_rank):
             "bulk_ms_per_launch": r["bulk_ms_per_launch"], "boundary_ms_per_launch": r["boundary_ms_per_launch"],
             "bulk_gbs": r["bulk_gbs"], "roofline_frac": r["bulk_gbs"] / peak if r["bulk_gbs"] else None,
             "bytes_per_cell_update": r["bytes_per_cell"], "clocks": r["clocks"], "stats_after": r["stats_after"],
+            "closure_coverage": r["closure_coverage"],
         }
     line = {
         "metric": METRIC, "value": value, "unit": "GLUPS", "n_gpus": world, "steps": args.steps,

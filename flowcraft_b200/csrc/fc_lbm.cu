@@ -773,7 +773,8 @@ int fc_lbm_closure_probe(fc_lbm* h, float* out, uint8_t* in_range, size_t cells)
     FC_TRY(h, cudaMalloc(&d_out, h->g.n * 5 * sizeof(float)), "alloc probe");
     cudaError_t e = cudaMalloc(&d_rng, h->g.n);
     if (e == cudaSuccess)
-        e = fc::launch_closure_probe(h->q, h->storage, h->pop[h->cur], h->g, h->closure, d_out, d_rng, h->stream);
+        e = fc::launch_closure_probe(h->q, h->storage, h->pop[h->cur], h->g, h->closure, d_out, d_rng, nullptr,
+                                     h->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(out, d_out, h->g.n * 5 * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(in_range, d_rng, h->g.n, cudaMemcpyDeviceToHost, h->stream);
@@ -782,6 +783,27 @@ int fc_lbm_closure_probe(fc_lbm* h, float* out, uint8_t* in_range, size_t cells)
     if (d_rng) cudaFree(d_rng);
     h->launches++;
     return rc;
+}
+
+int fc_lbm_closure_coverage(fc_lbm* h, uint64_t* cells_in_range, uint64_t* warps_with_mlp) {
+    FC_RC(check_ready(h));
+    if (!h->closure_on) return fail(h, FC_LBM_ERR_NOT_INITIALIZED, "no learned closure set");
+    if (!cells_in_range || !warps_with_mlp) return FC_LBM_ERR_INVALID_ARG;
+    DeviceGuard dg(h->device);
+    unsigned long long* d = reinterpret_cast<unsigned long long*>(h->d_stats_result);  // 2 slots, reused
+    FC_TRY(h, cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), h->stream), "clear counts");
+    FC_TRY(h, fc::launch_closure_probe(h->q, h->storage, h->pop[h->cur], h->g, h->closure, nullptr, nullptr, d,
+                                       h->stream),
+           "closure coverage");
+    h->launches++;
+    FC_TRY(h, cudaMemcpyAsync(h->h_stage, d, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream),
+           "coverage download");
+    FC_RC(wait_stream(h, kTransferTimeoutMs));
+    unsigned long long r[2];
+    std::memcpy(r, h->h_stage, sizeof(r));
+    *cells_in_range = r[0];
+    *warps_with_mlp = r[1];
+    return FC_LBM_OK;
 }
 
 int fc_lbm_wall_distance(fc_lbm* h, uint8_t* out, size_t cells) {

@@ -119,7 +119,7 @@ cudaError_t launch_bulk_pull_learned(int q, int storage, const void* fin, void* 
                                      const Geom& g, const StepParams& p, int z0, int zc, int* diverged,
                                      cudaStream_t s, int* launched, const ClosureDev& cl);
 cudaError_t launch_closure_probe(int q, int storage, const void* f, const Geom& g, const ClosureDev& cl, float* out,
-                                 uint8_t* in_range, cudaStream_t s);
+                                 uint8_t* in_range, unsigned long long* counts, cudaStream_t s);
 
 cudaError_t launch_bulk_pull(int q, int storage, const void* fin, void* fout, const uint32_t* bulk_bits,
                              const Geom& g, const StepParams& p, int z0, int zc, int* diverged, cudaStream_t s,

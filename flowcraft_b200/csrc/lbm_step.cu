@@ -467,7 +467,11 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned(const 
     closure_pack_inputs(cl, xa0, xa1, xa2, (float)(wd & 0xffu) * 0.0625f, in);
     closure_pack_inputs(cl, xb0, xb1, xb2, (float)(wd >> 8) * 0.0625f, in + 4);
     __syncwarp();
-    const float2 nu = closure_warp_mlp(cl.frag, s_in[threadIdx.y], s_out[threadIdx.y]);
+    // A cell outside the training range takes the Smagorinsky value, so a
+    // warp with no cell in range has no use for the MLP and skips it (the
+    // result is the same); the vote keeps the branch warp-uniform.
+    float2 nu = make_float2(0.0f, 0.0f);
+    if (__any_sync(0xffffffffu, la || lb)) nu = closure_warp_mlp(cl.frag, s_in[threadIdx.y], s_out[threadIdx.y]);
     if (!pair) return;
     float2 gr;
     gr.x = la ? (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.x, p.tau))) * 4.5f : sga;
@@ -491,10 +495,13 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned(const 
 // as stored (no streaming): the same device code as the fused kernels, for
 // checking the inference against a CPU evaluation. Two cells per lane.
 // out[5*c .. 5*c+4] = inputs 0-3 and nu_t; in_range[c] = 1 when the learned
-// value is used.
+// value is used. With out == nullptr it only counts, into counts[0] the
+// cells in range and into counts[1] the 64-cell warps with any cell in range
+// (the warps that run the MLP in a step).
 template <int Q, class S>
 __global__ void __launch_bounds__(128) k_closure_probe(const typename S::T* __restrict__ f, Geom g, ClosureDev cl,
-                                                       float* __restrict__ out, uint8_t* __restrict__ in_range) {
+                                                       float* __restrict__ out, uint8_t* __restrict__ in_range,
+                                                       unsigned long long* __restrict__ counts) {
     static_assert(!S::kExact, "the learned closure runs on the 16-bit offset formats");
     __shared__ uint32_t s_in[4][32 * 8];
     __shared__ float2 s_out[4][32];
@@ -516,6 +523,16 @@ __global__ void __launch_bounds__(128) k_closure_probe(const typename S::T* __re
     xa[3] = ha ? (float)cl.wall[c] * 0.0625f : 0.0f;
     xb[3] = hb ? (float)cl.wall[c + 1] * 0.0625f : 0.0f;
     const int warp = threadIdx.x >> 5;
+    if (!out) {
+        const bool ra = ha && closure_in_range(cl, xa[0], xa[1], xa[2]);
+        const bool rb = hb && closure_in_range(cl, xb[0], xb[1], xb[2]);
+        const unsigned cells = __popc(__ballot_sync(0xffffffffu, ra)) + __popc(__ballot_sync(0xffffffffu, rb));
+        if ((threadIdx.x & 31) == 0 && cells) {
+            atomicAdd(counts, (unsigned long long)cells);
+            atomicAdd(counts + 1, 1ull);
+        }
+        return;
+    }
     uint32_t* in = &s_in[warp][(threadIdx.x & 31) * 8];
     closure_pack_inputs(cl, xa[0], xa[1], xa[2], xa[3], in);
     closure_pack_inputs(cl, xb[0], xb[1], xb[2], xb[3], in + 4);
@@ -701,14 +718,15 @@ __global__ void __launch_bounds__(128) k_boundary_pull_learned(const typename S:
     float x0, x1, x2;
     closure_invariants(mo.pxx.x, mo.pyy.x, mo.pzz.x, mo.pxy.x, mo.pxz.x, mo.pyz.x, mo.pp.x, mo.inv.x, x0, x1, x2);
     const float x3 = fluid ? (float)__ldg(cl.wall + c) * 0.0625f : 0.0f;
-    const bool lin = closure_in_range(cl, x0, x1, x2);
+    const bool lin = fluid && closure_in_range(cl, x0, x1, x2);
     const float sg = smagorinsky_g(mo.pp.x, mo.rho.x, mo.inv.x, p.tau, p.cs);
     const int warp = threadIdx.x >> 5;
     uint32_t* in = &s_in[warp][(threadIdx.x & 31) * 8];
     closure_pack_inputs(cl, x0, x1, x2, x3, in);
     closure_pack_inputs(cl, 0.0f, 0.0f, 0.0f, 0.0f, in + 4);
     __syncwarp();
-    const float2 nu = closure_warp_mlp(cl.frag, s_in[warp], s_out[warp]);
+    float2 nu = make_float2(0.0f, 0.0f);  // warps with no cell in range skip the MLP
+    if (__any_sync(0xffffffffu, lin)) nu = closure_warp_mlp(cl.frag, s_in[warp], s_out[warp]);
     if (!fluid) return;
     const float gx = lin ? (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.x, p.tau))) * 4.5f : sg;
     relax2<Q>(h, mo, make_float2(gx, gx));
@@ -830,13 +848,13 @@ static cudaError_t boundary_learned_t(const void* fin, void* fout, const Boundar
 
 template <int Q, class S>
 static cudaError_t closure_probe_t(const void* f, const Geom& g, const ClosureDev& cl, float* out, uint8_t* in_range,
-                                   cudaStream_t s) {
+                                   unsigned long long* counts, cudaStream_t s) {
     if constexpr (S::kExact) {
         return cudaErrorNotSupported;
     } else {
         const size_t pairs = (g.n + 1) / 2;
         k_closure_probe<Q, S><<<(unsigned)((pairs + 127) / 128), 128, 0, s>>>((const typename S::T*)f, g, cl, out,
-                                                                              in_range);
+                                                                              in_range, counts);
         return cudaGetLastError();
     }
 }
@@ -880,8 +898,8 @@ cudaError_t launch_boundary_pull_learned(int q, int storage, const void* fin, vo
 }
 
 cudaError_t launch_closure_probe(int q, int storage, const void* f, const Geom& g, const ClosureDev& cl, float* out,
-                                 uint8_t* in_range, cudaStream_t s) {
-    FC_DISPATCH(q, storage, closure_probe_t, f, g, cl, out, in_range, s);
+                                 uint8_t* in_range, unsigned long long* counts, cudaStream_t s) {
+    FC_DISPATCH(q, storage, closure_probe_t, f, g, cl, out, in_range, counts, s);
 }
 
 }  // namespace fc

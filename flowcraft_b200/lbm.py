@@ -149,6 +149,7 @@ SIGNATURES = {
     "fc_lbm_set_closure": (ctypes.c_int, [_P, ctypes.POINTER(_Closure)]),
     "fc_lbm_closure_probe": (ctypes.c_int, [_P, _FP, ctypes.POINTER(ctypes.c_uint8), _SZ]),
     "fc_lbm_wall_distance": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint8), _SZ]),
+    "fc_lbm_closure_coverage": (ctypes.c_int, [_P, _U64P, _U64P]),
     "fc_lbm_closure_samples": (ctypes.c_int, [_P, ctypes.c_float, _P, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "fc_lbm_mlp_forward": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P, _P]),
     "fc_lbm_mlp_grad": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int64, _P, _P, _P, _P]),
@@ -460,6 +461,15 @@ class LbmSolver:
         self._check(self._lib.fc_lbm_closure_samples(self._h, float(filterWidth), out.data_ptr(), out.shape[0],
                                                      ctypes.byref(cnt)), "ClosureSamples")
         return out[:n]
+
+    def ClosureCoverage(self) -> dict:
+        """Cells in the closure's training range and warps that run its MLP."""
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(self._lib.fc_lbm_closure_coverage(self._h, ctypes.byref(a), ctypes.byref(b)), "ClosureCoverage")
+        n = self.CellCount()
+        warps = (n + 63) // 64
+        return {"cells_in_range": int(a.value), "cell_fraction": a.value / max(n, 1),
+                "warps_with_mlp": int(b.value), "warp_fraction": b.value / max(warps, 1)}
 
     def WallDistance(self) -> np.ndarray:
         """The closure's wall-distance input, bytes in 1/16-cell steps."""

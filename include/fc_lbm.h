@@ -270,6 +270,12 @@ FC_LBM_API int fc_lbm_set_closure(fc_lbm* h, const fc_closure* c);
  * in_range[c] = 1 where the learned nu_t is used. Host arrays; cells must be
  * nx*ny*nz. For checking the inference. */
 FC_LBM_API int fc_lbm_closure_probe(fc_lbm* h, float* out, uint8_t* in_range, size_t cells);
+/* How much of the current state the closure covers: the cells whose inputs
+ * are in the training range, and the groups of 64 consecutive cells that
+ * hold at least one of them. When nx is a multiple of 64 those groups are the
+ * step kernel's warps, and the count is the number of warps that evaluate
+ * the MLP in a step; the others keep Smagorinsky and skip it. Blocking. */
+FC_LBM_API int fc_lbm_closure_coverage(fc_lbm* h, uint64_t* cells_in_range, uint64_t* warps_with_mlp);
 /* The wall-distance input (1/16-cell steps, 255 = 15.94 cells or more). */
 FC_LBM_API int fc_lbm_wall_distance(fc_lbm* h, uint8_t* out, size_t cells);
 

@@ -101,6 +101,12 @@ def test_probe_inputs_and_inference(gpu, oracle_built, q):
     err = np.abs(nu[sel] - ref[sel]) / (np.abs(ref[sel]) + 1e-6)
     print(f"D3Q{q}: nu_t mean {ref[sel].mean():.3e}, rel err median {np.median(err):.2e} max {err.max():.2e}")
     assert np.median(err) < 1e-3 and np.quantile(err, 0.999) < 3e-2
+    # the coverage counters agree with the probe
+    cov = sim.s.ClosureCoverage()
+    assert cov["cells_in_range"] == int(in_range.sum())
+    n = len(in_range)
+    groups = np.pad(in_range, (0, (-n) % 64)).reshape(-1, 64).any(axis=1)
+    assert cov["warps_with_mlp"] == int(groups.sum())
 
 
 @pytest.mark.parametrize("storage,tol,margin", [("FP16_OFFSET", 3e-4, 5.0), ("BF16_OFFSET", 2e-3, 2.0)])
