@@ -48,6 +48,11 @@ CONFIGS = {
     # the plain-FP32 parity lattice: 128x64x64, sphere r=10, Re=100
     "c1": dict(nx=128, ny=64, nz=64, geom="sphere", u=0.05, re=100.0, lref=20.0, cs=0.1,
                desc="D3Q19 128x64x64 (524k cells), sphere r=10 at (40,32,32), U=0.05, Re=100 (tau=0.53), Cs=0.1"),
+    # the batched-throughput set: 16 NACA 2412 lattices of seeded sizes 64x32x32 .. 256x128x128
+    "c3": dict(nx=0, ny=0, nz=0, geom="batch", u=0.0, re=0.0, lref=0.0, cs=0.1,
+               desc="D3Q19 batch of 16 NACA 2412 wing lattices, sizes 64x32x32..256x128x128 (2:1:1) drawn with seed "
+                    "20261203, chord 0.375 nx, AoA -8..14 deg, U 0.04-0.08, Re 1e3-2e4, FP16 offset, Smagorinsky "
+                    "Cs=0.1, one persistent launch per step over all lattices (autotuned block shape)"),
     # the precision-study lattice size: 384x192x192 NACA 0012 wing, chord 96, 4 deg
     "c2": dict(nx=384, ny=192, nz=192, geom="naca0012", u=0.06, re=1e4, lref=96.0, cs=0.1,
                desc="D3Q19 384x192x192 (14.2M cells), NACA 0012 wing chord 96 span 128 at 4 deg, U=0.06, "
@@ -355,8 +360,70 @@ def run_e2e(args, cfg, solid, sdf, variant, dev_index):
                      "ProbeSliceHealth) + ReadbackStats + ReadbackFieldRange(all z)"}
 
 
+def run_batch(args, cfg, rank, world, local_rank):
+    """The c3 set: every rank steps its own batch of 16 lattices."""
+    import torch
+
+    from flowcraft_b200.batch import LbmBatch
+    from flowcraft_b200.sweep import c3_lattices, make_members
+    dist_on = world > 1
+    torch.cuda.set_device(local_rank)
+    mem = make_members(c3_lattices(), "FP16_OFFSET", cfg["cs"], local_rank)
+    solvers = [m[0] for m in mem]
+    cells = sum(s.CellCount() for s in solvers)
+    b = LbmBatch(solvers)
+    tuned = b.Tune(4)
+    b.Step(2 * args.warmup)
+    torch.cuda.synchronize()
+    barrier_sync(dist_on)
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    steps = args.steps + (args.steps & 1)
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    # the batch runs on its own stream, ordered after and before the members'
+    # streams; events on the first member's stream bracket it
+    s0 = torch.cuda.ExternalStream(solvers[0].Stream())
+    start.record(s0)
+    b.Step(steps)
+    stop.record(s0)
+    stop.synchronize()
+    ms = start.elapsed_time(stop)
+    clocks = sampler.stop() if sampler else None
+    # the same members stepped one after another on one stream, for contrast
+    seq = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    seq_start = torch.cuda.Event(enable_timing=True)
+    seq_stop = torch.cuda.Event(enable_timing=True)
+    seq_start.record(seq)
+    for s in solvers:
+        s.Step(seq.cuda_stream, steps)
+    seq_stop.record(seq)
+    seq_stop.synchronize()
+    seq_ms = seq_start.elapsed_time(seq_stop)
+    barrier_sync(dist_on)
+    ms = allreduce_max(ms, dist_on)
+    diverged = [s.HasDiverged() for s in solvers]
+    b.close()
+    if rank != 0:
+        return 0
+    value = world * cells * steps / (ms / 1e3) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": "GLUPS", "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic: analytic NACA 2412 lattices on the device",
+            "config": {"workload": cfg["desc"], "lattices": len(solvers), "cells": cells,
+                       "sizes": [m[1]["nx"] for m in mem], "autotune": tuned,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "diverged": any(diverged), "gpu_launches": 2 * steps, "clocks": clocks,
+            "sequential": {"glups": world * cells * steps / (seq_ms / 1e3) / 1e9, "ms_per_step": seq_ms / steps,
+                           "how": "the same lattices stepped one after another on one stream with LbmSolver.Step"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ours(args, cfg, rank, world, local_rank):
     import torch
+    if cfg["geom"] == "batch":
+        return run_batch(args, cfg, rank, world, local_rank)
     dist_on = world > 1
     torch.cuda.set_device(local_rank)
     dev_index = local_rank

@@ -1027,4 +1027,317 @@ int fc_lbm_load_populations(fc_lbm* h, const float* in, size_t count) {
     return wait_stream(h, kTransferTimeoutMs);
 }
 
+// ---- batches: many lattices stepped together (fc_lbm_batch) ----
+}  // extern "C"
+
+struct fc_lbm_batch {
+    std::vector<fc_lbm*> m;
+    int device = 0, q = 19, storage = FC_STORAGE_FP32, model = FC_LATTICE_D3Q19;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev = nullptr;
+    fc::BatchLattice* d_lat = nullptr;
+    std::vector<fc::BatchLattice> h_lat;
+    unsigned long long total = 0;   // bulk work items
+    unsigned long long btotal = 0;  // boundary-list entries
+    int rows = 8, mult = 1, grid = 0;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uint64_t> sig;  // member state the descriptors and the graph were built for
+    std::string err;
+};
+
+namespace {
+
+constexpr int kBatchRows[3] = {4, 8, 16};
+constexpr int kBatchMult[2] = {1, 2};
+
+int bfail(fc_lbm_batch* b, int code, const std::string& msg) {
+    b->err = msg;
+    return code;
+}
+
+int bcuda(fc_lbm_batch* b, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return FC_LBM_OK;
+    return bfail(b, e == cudaErrorMemoryAllocation ? FC_LBM_ERR_OUT_OF_MEMORY : FC_LBM_ERR_CUDA,
+                 std::string(what) + ": " + cudaGetErrorName(e));
+}
+
+#define FB_TRY(b, expr, what)                          \
+    do {                                               \
+        const int _rc = bcuda((b), (expr), (what));    \
+        if (_rc != FC_LBM_OK) return _rc;              \
+    } while (0)
+
+uint64_t fbits64(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+}
+
+std::vector<uint64_t> batch_signature(const fc_lbm_batch* b) {
+    std::vector<uint64_t> v{(uint64_t)b->rows, (uint64_t)b->mult};
+    for (const fc_lbm* h : b->m) {
+        v.push_back((uint64_t)(uintptr_t)h->pop[0]);
+        v.push_back((uint64_t)(uintptr_t)h->pop[1]);
+        v.push_back((uint64_t)h->cur);
+        v.push_back(fbits64(h->params.tau) | (fbits64(h->params.inlet_velocity) << 32));
+        v.push_back(fbits64(h->params.smagorinsky_cs) | ((uint64_t)h->params.reverse_flow << 32) |
+                    ((uint64_t)h->params.free_slip_y << 33) | ((uint64_t)h->params.free_slip_z << 34));
+    }
+    return v;
+}
+
+// Descriptors of every member for the current block shape, uploaded.
+int batch_build(fc_lbm_batch* b) {
+    const size_t elem = b->storage == FC_STORAGE_FP32 ? 4 : 2;
+    b->h_lat.assign(b->m.size(), fc::BatchLattice{});
+    unsigned long long first = 0, bfirst = 0;
+    for (size_t k = 0; k < b->m.size(); ++k) {
+        fc_lbm* h = b->m[k];
+        fc::BatchLattice& d = b->h_lat[k];
+        d.g = h->g;
+        d.p = step_params(h);
+        for (int side = 0; side < 2; ++side) {
+            const char* in = static_cast<const char*>(h->pop[side]);
+            char* out = static_cast<char*>(h->pop[1 - side]);
+            for (int i = 0; i < b->q; ++i) {
+                const long long off = (long long)(b->q == 19 ? fc::Lattice<19>::ex(i) : fc::Lattice<15>::ex(i)) +
+                                      (long long)(b->q == 19 ? fc::Lattice<19>::ey(i) : fc::Lattice<15>::ey(i)) *
+                                          h->g.nx +
+                                      (long long)(b->q == 19 ? fc::Lattice<19>::ez(i) : fc::Lattice<15>::ez(i)) *
+                                          h->g.nxy;
+                d.pp[side].src[i] = in + ((long long)i * (long long)h->g.n - off) * (long long)elem;
+                d.pp[side].dst[i] = out + (size_t)i * h->g.n * elem;
+            }
+        }
+        d.pop[0] = h->pop[0];
+        d.pop[1] = h->pop[1];
+        const uint32_t b0 = h->z_begin[0], b1 = h->z_begin[(size_t)h->g.nz];
+        d.bl = fc::BoundaryList{h->d_cells ? h->d_cells + b0 : nullptr, h->d_links ? h->d_links + b0 : nullptr,
+                                h->d_coef_off ? h->d_coef_off + b0 : nullptr, h->d_coef};
+        d.bnd_first = bfirst;
+        bfirst += b1 > b0 ? b1 - b0 : 0;
+        d.bits = h->d_bulk_bits;
+        d.diverged = h->d_diverged;
+        d.gx = (h->g.nx + 63) / 64;
+        d.gy = (h->g.ny + b->rows - 1) / b->rows;
+        d.first = first;
+        d.cur = h->cur;
+        first += (unsigned long long)d.gx * d.gy * h->g.nz;
+    }
+    b->total = first;
+    b->btotal = bfirst;
+    const int resident = fc::bulk_batch_resident(b->q, b->storage, b->rows);
+    int sms = 0;
+    FB_TRY(b, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device), "SM count");
+    if (resident <= 0) return bfail(b, FC_LBM_ERR_CUDA, "batch kernel occupancy query failed");
+    b->grid = sms * resident * b->mult;
+    FB_TRY(b, cudaMemcpyAsync(b->d_lat, b->h_lat.data(), b->h_lat.size() * sizeof(fc::BatchLattice),
+                              cudaMemcpyHostToDevice, b->stream),
+           "upload batch descriptors");
+    return FC_LBM_OK;
+}
+
+// One step of every member (parity relative to the members' current sets).
+int batch_step_direct(fc_lbm_batch* b, int parity) {
+    FB_TRY(b, fc::launch_bulk_batch(b->q, b->storage, b->rows, b->d_lat, (int)b->m.size(), b->total, parity, b->grid,
+                                    b->stream),
+           "batch bulk step");
+    FB_TRY(b, fc::launch_boundary_batch(b->q, b->storage, b->d_lat, (int)b->m.size(), b->btotal, parity, b->stream),
+           "batch boundary step");
+    return FC_LBM_OK;
+}
+
+int batch_prepare(fc_lbm_batch* b, bool want_graph) {
+    const std::vector<uint64_t> sig = batch_signature(b);
+    if (sig != b->sig) {
+        if (b->exec) {
+            cudaGraphExecDestroy(b->exec);
+            b->exec = nullptr;
+        }
+        FC_RC(batch_build(b));
+        b->sig = sig;
+    }
+    if (want_graph && !b->exec) {
+        // two steps, one of each parity: a replay leaves every member on its own set
+        cudaGraph_t graph = nullptr;
+        FB_TRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        int rc = batch_step_direct(b, 0);
+        if (rc == FC_LBM_OK) rc = batch_step_direct(b, 1);
+        const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+        if (rc != FC_LBM_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        FB_TRY(b, e, "end capture");
+        const cudaError_t ie = cudaGraphInstantiate(&b->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        FB_TRY(b, ie, "instantiate graph");
+    }
+    return FC_LBM_OK;
+}
+
+int batch_check(fc_lbm_batch* b) {
+    for (fc_lbm* h : b->m)
+        if (!h->valid || h->device != b->device || h->q != b->q || h->storage != b->storage || h->closure_on ||
+            h->g.nx % 2 != 0)
+            return bfail(b, FC_LBM_ERR_INVALID_ARG, "a batch member changed (re-initialized, closure set or shut down)");
+    return FC_LBM_OK;
+}
+
+int batch_enter(fc_lbm_batch* b) {
+    for (fc_lbm* h : b->m) {
+        FB_TRY(b, cudaEventRecord(b->ev, h->stream), "member event");
+        FB_TRY(b, cudaStreamWaitEvent(b->stream, b->ev, 0), "wait member");
+    }
+    return FC_LBM_OK;
+}
+
+int batch_leave(fc_lbm_batch* b) {
+    FB_TRY(b, cudaEventRecord(b->ev, b->stream), "batch event");
+    for (fc_lbm* h : b->m) FB_TRY(b, cudaStreamWaitEvent(h->stream, b->ev, 0), "member wait");
+    return FC_LBM_OK;
+}
+
+int batch_wait(fc_lbm_batch* b) {
+    FB_TRY(b, cudaEventRecord(b->ev, b->stream), "batch event");
+    const auto t0 = std::chrono::steady_clock::now();
+    int sleep_us = 20;
+    for (;;) {
+        const cudaError_t q = cudaEventQuery(b->ev);
+        if (q == cudaSuccess) return FC_LBM_OK;
+        if (q != cudaErrorNotReady) return bcuda(b, q, "batch wait");
+        if (std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(kTransferTimeoutMs))
+            return bfail(b, FC_LBM_ERR_TIMEOUT, "batch wait timed out");
+        std::this_thread::sleep_for(std::chrono::microseconds(sleep_us));
+        if (sleep_us < 2000) sleep_us *= 2;
+    }
+}
+
+void batch_advance(fc_lbm_batch* b, int n, uint64_t launches_per_step) {
+    for (fc_lbm* h : b->m) {
+        if (n & 1) h->cur = 1 - h->cur;
+        h->steps_since_reset += (uint64_t)n;
+        h->launches += (uint64_t)n * launches_per_step;  // shared launches, counted in every member
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int fc_lbm_batch_create(fc_lbm* const* members, int32_t count, fc_lbm_batch** out) {
+    if (!out) return FC_LBM_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (!members || count <= 0 || count > 4096) return FC_LBM_ERR_INVALID_ARG;
+    fc_lbm* h0 = members[0];
+    if (!h0 || !h0->valid) return FC_LBM_ERR_NOT_INITIALIZED;
+    for (int k = 0; k < count; ++k) {
+        fc_lbm* h = members[k];
+        if (!h || !h->valid) return FC_LBM_ERR_NOT_INITIALIZED;
+        if (h->device != h0->device || h->q != h0->q || h->storage != h0->storage) return FC_LBM_ERR_INVALID_ARG;
+        if (h->g.nx % 2 != 0 || h->closure_on) return FC_LBM_ERR_UNSUPPORTED;
+        for (int j = 0; j < k; ++j)
+            if (members[j] == h) return FC_LBM_ERR_INVALID_ARG;
+    }
+    auto* b = new (std::nothrow) fc_lbm_batch();
+    if (!b) return FC_LBM_ERR_OUT_OF_MEMORY;
+    b->m.assign(members, members + count);
+    b->device = h0->device;
+    b->q = h0->q;
+    b->storage = h0->storage;
+    b->model = h0->model;
+    DeviceGuard dg(b->device);
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_lat, (size_t)count * sizeof(fc::BatchLattice));
+    if (e != cudaSuccess) {
+        fc_lbm_batch_destroy(b);
+        return e == cudaErrorMemoryAllocation ? FC_LBM_ERR_OUT_OF_MEMORY : FC_LBM_ERR_CUDA;
+    }
+    *out = b;
+    return FC_LBM_OK;
+}
+
+void fc_lbm_batch_destroy(fc_lbm_batch* b) {
+    if (!b) return;
+    DeviceGuard dg(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->d_lat) cudaFree(b->d_lat);
+    if (b->ev) cudaEventDestroy(b->ev);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+const char* fc_lbm_batch_last_error(const fc_lbm_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+int fc_lbm_batch_step(fc_lbm_batch* b, int32_t n) {
+    if (!b || n < 0) return FC_LBM_ERR_INVALID_ARG;
+    FC_RC(batch_check(b));
+    if (n == 0) return FC_LBM_OK;
+    DeviceGuard dg(b->device);
+    FC_RC(batch_enter(b));
+    FC_RC(batch_prepare(b, n >= 2));
+    for (int k = 0; k + 1 < n; k += 2) FB_TRY(b, cudaGraphLaunch(b->exec, b->stream), "graph launch");
+    if (n & 1) FC_RC(batch_step_direct(b, 0));
+    batch_advance(b, n, 2);
+    return batch_leave(b);
+}
+
+int fc_lbm_batch_config(fc_lbm_batch* b, int32_t rows, int32_t grid_mult) {
+    if (!b) return FC_LBM_ERR_INVALID_ARG;
+    if ((rows != 4 && rows != 8 && rows != 16) || (grid_mult != 1 && grid_mult != 2))
+        return bfail(b, FC_LBM_ERR_INVALID_ARG, "rows must be 4, 8 or 16 and grid_mult 1 or 2");
+    b->rows = rows;
+    b->mult = grid_mult;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_batch_tune(fc_lbm_batch* b, int32_t steps, int32_t* rows, int32_t* grid_mult, float* ms_per_step) {
+    if (!b || steps < 1) return FC_LBM_ERR_INVALID_ARG;
+    FC_RC(batch_check(b));
+    DeviceGuard dg(b->device);
+    const int timed = steps + (steps & 1);  // even: every member ends on its own set
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    FB_TRY(b, cudaEventCreate(&t0), "timing event");
+    if (cudaEventCreate(&t1) != cudaSuccess) {
+        cudaEventDestroy(t0);
+        return bfail(b, FC_LBM_ERR_CUDA, "timing event");
+    }
+    int rc = batch_enter(b);
+    float best = 1e30f;
+    int best_r = 8, best_m = 1, idx = 0;
+    for (int r : kBatchRows)
+        for (int mu : kBatchMult) {
+            if (rc != FC_LBM_OK) break;
+            b->rows = r;
+            b->mult = mu;
+            rc = batch_prepare(b, false);
+            for (int k = 0; k < 2 && rc == FC_LBM_OK; ++k) rc = batch_step_direct(b, k);  // warm-up
+            if (rc == FC_LBM_OK) rc = bcuda(b, cudaEventRecord(t0, b->stream), "timing");
+            for (int k = 0; k < timed && rc == FC_LBM_OK; ++k) rc = batch_step_direct(b, k & 1);
+            if (rc == FC_LBM_OK) rc = bcuda(b, cudaEventRecord(t1, b->stream), "timing");
+            if (rc == FC_LBM_OK) rc = batch_wait(b);
+            float ms = 0.0f;
+            if (rc == FC_LBM_OK) rc = bcuda(b, cudaEventElapsedTime(&ms, t0, t1), "timing");
+            const float per = ms / (float)timed;
+            if (ms_per_step) ms_per_step[idx] = per;
+            if (rc == FC_LBM_OK && per < best) {
+                best = per;
+                best_r = r;
+                best_m = mu;
+            }
+            ++idx;
+            batch_advance(b, timed + 2, 2);
+        }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    b->rows = best_r;
+    b->mult = best_m;
+    if (rows) *rows = best_r;
+    if (grid_mult) *grid_mult = best_m;
+    if (rc == FC_LBM_OK) rc = batch_leave(b);
+    return rc;
+}
+
 }  // extern "C"

@@ -121,6 +121,38 @@ cudaError_t launch_bulk_pull_learned(int q, int storage, const void* fin, void* 
 cudaError_t launch_closure_probe(int q, int storage, const void* f, const Geom& g, const ClosureDev& cl, float* out,
                                  uint8_t* in_range, unsigned long long* counts, cudaStream_t s);
 
+// One lattice of a batch (fc_lbm_batch): everything the persistent bulk
+// kernel needs, in device memory. pp[k] are the plane pointers of a step that
+// reads pop[k] and writes pop[1 - k]; a step of parity `par` reads
+// pop[cur ^ par]. Work items (tiles of 64 x ROWS cells of one z layer) of
+// lattice k are first .. first + gx * gy * nz - 1.
+struct BatchLattice {
+    Geom g;
+    StepParams p;
+    PlanePtrs pp[2];
+    const void* pop[2];
+    const uint32_t* bits;
+    int* diverged;
+    unsigned long long first;      // first bulk work item
+    unsigned long long bnd_first;  // first entry in the concatenated boundary lists
+    BoundaryList bl;
+    int gx, gy;
+    int cur;
+    int pad;
+};
+
+// The persistent bulk kernel of a batch (all lattices even nx, one model and
+// storage): `grid` blocks of 32 x rows threads loop over `total` work items.
+// rows is 4, 8 or 16.
+cudaError_t launch_bulk_batch(int q, int storage, int rows, const BatchLattice* lat, int nlat,
+                              unsigned long long total, int parity, int grid, cudaStream_t s);
+// The boundary-list entries of every lattice of a batch in one launch
+// (`total` = the sum of the lattices' list lengths).
+cudaError_t launch_boundary_batch(int q, int storage, const BatchLattice* lat, int nlat, unsigned long long total,
+                                  int parity, cudaStream_t s);
+// Blocks of the batch kernel resident per SM (occupancy), or 0.
+int bulk_batch_resident(int q, int storage, int rows);
+
 cudaError_t launch_bulk_pull(int q, int storage, const void* fin, void* fout, const uint32_t* bulk_bits,
                              const Geom& g, const StepParams& p, int z0, int zc, int* diverged, cudaStream_t s,
                              int* launched);

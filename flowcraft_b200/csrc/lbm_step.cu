@@ -29,6 +29,7 @@
 namespace fc {
 
 constexpr int kBulkRows = 8;  // block = 32 x-lanes x 8 rows
+constexpr int kBatchChunk = 8;  // consecutive tiles a block of the batch kernel takes at a time
 
 template <int Q>
 __device__ __forceinline__ long long link_offset(int i, const Geom& g) {
@@ -550,6 +551,145 @@ __global__ void __launch_bounds__(128) k_closure_probe(const typename S::T* __re
     }
 }
 
+// The bulk step of many lattices in one persistent launch over a work-list of
+// tiles (64 x ROWS cells of one z layer) spanning every lattice of a batch.
+// Blocks stride over chunks of kBatchChunk consecutive tiles (block b takes
+// chunks b, b + G, b + 2G, ...), which interleaves cheap and costly tiles
+// across blocks. A block finds a tile's lattice by binary search over the
+// lattices' first items and keeps that lattice's descriptor (geometry, step
+// parameters, plane pointers) in shared memory while consecutive tiles stay
+// in it, so it reloads it at most once per chunk. The per-tile work and arithmetic are those of k_bulk_pairs, so
+// a batch step is bit-identical to stepping each lattice alone.
+template <int Q, class S, int ROWS>
+__global__ void __launch_bounds__(32 * ROWS, 32 / ROWS) k_bulk_pairs_batch(const BatchLattice* __restrict__ lat,
+                                                                           int nlat, unsigned long long total,
+                                                                           int parity) {
+    using L = Lattice<Q>;
+    using T = typename S::T;
+    __shared__ BatchLattice sl;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    int cur_lat = -1;
+    const unsigned long long chunks = (total + kBatchChunk - 1) / kBatchChunk;
+    for (unsigned long long ch = blockIdx.x; ch < chunks; ch += gridDim.x)
+    for (unsigned long long w = ch * kBatchChunk; w < min(total, (ch + 1) * kBatchChunk); ++w) {
+        int lo = 0, hi = nlat - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(&lat[mid].first) <= w) lo = mid;
+            else hi = mid - 1;
+        }
+        if (lo != cur_lat) {  // the same lattice for every thread of the block
+            __syncthreads();
+            const int* srcw = reinterpret_cast<const int*>(lat + lo);
+            int* dstw = reinterpret_cast<int*>(&sl);
+            for (int k = tid; k < (int)(sizeof(BatchLattice) / 4); k += 32 * ROWS) dstw[k] = __ldg(srcw + k);
+            __syncthreads();
+            cur_lat = lo;
+        }
+        const Geom& g = sl.g;
+        const StepParams& p = sl.p;
+        const int side = sl.cur ^ parity;
+        const PlanePtrs& pp = sl.pp[side];
+        const T* __restrict__ fin = static_cast<const T*>(sl.pop[side]);
+        T* __restrict__ fout = static_cast<T*>(const_cast<void*>(sl.pop[side ^ 1]));
+        const unsigned long long local = w - sl.first;
+        const int bx = (int)(local % (unsigned)sl.gx);
+        const unsigned long long t = local / (unsigned)sl.gx;
+        const int y = (int)(t % (unsigned)sl.gy) * ROWS + threadIdx.y;
+        const int z = (int)(t / (unsigned)sl.gy);
+        if (y >= g.ny) continue;
+        const size_t row = (size_t)z * g.ny + y;
+        const int k = 2 * threadIdx.x;
+        const int wd = 2 * bx + (k >> 5);
+        const uint32_t bits = wd < g.wpr ? __ldg(sl.bits + row * g.wpr + wd) : 0u;
+        const int x = 64 * bx + k;
+        unsigned pair = (bits >> (k & 31)) & 3u;
+        unsigned plane = 0;
+        if (x == 0) {
+            plane |= pair & 1u;
+            pair &= ~1u;
+        }
+        if (x + 1 == g.nx - 1) {
+            plane |= pair & 2u;
+            pair &= ~2u;
+        }
+        if (!(pair | plane)) continue;
+        const uint32_t c = (uint32_t)(row * g.nx + x);
+        const bool face = (y == 0) | (y == g.ny - 1) | (z == 0) | (z == g.nz - 1);
+        const bool edge = (bx == 0) | (64 * bx + 64 >= g.nx);
+        float2 v[Q];
+        if (!face && !edge) {
+            if (pair != 3u) {
+                const uint32_t cc = pair == 1u ? c : c + 1u;
+                bulk_cell<Q, S, false>(fin, fout, g, p, x + (pair == 1u ? 0 : 1), y, z, cc, sl.diverged);
+                continue;
+            }
+            static_for<0, Q>([&](auto I) {
+                constexpr int i = decltype(I)::value;
+                const T* src = static_cast<const T*>(pp.src[i]);
+                if constexpr (S::kExact) {
+                    v[i] = L::ex(i) == 0 ? S::dec2(S::ld2(src + c), L::w(i))
+                                         : make_float2(S::dec(S::ld(src + c), L::w(i)),
+                                                       S::dec(S::ld(src + c + 1u), L::w(i)));
+                } else {
+                    v[i] = L::ex(i) == 0 ? S::raw2(S::ld2(src + c))
+                                         : make_float2(S::raw(S::ld(src + c)), S::raw(S::ld(src + c + 1u)));
+                }
+            });
+            if (collide_pair<Q, S>(v, p.tau, p.cs)) atomicOr(sl.diverged, 1);
+            static_for<0, Q>([&](auto I) {
+                constexpr int i = decltype(I)::value;
+                T* dst = static_cast<T*>(pp.dst[i]);
+                if constexpr (S::kExact)
+                    *reinterpret_cast<typename S::T2*>(dst + c) = S::enc2(v[i].x, v[i].y, L::w(i));
+                else
+                    *reinterpret_cast<typename S::T2*>(dst + c) = S::pack2(v[i].x, v[i].y);
+            });
+            continue;
+        }
+        if (plane) plane_cell<Q, S>(fin, fout, g, p, plane == 1u ? x : x + 1, plane == 1u ? c : (size_t)c + 1);
+        if (!pair) continue;
+        const bool va = pair & 1u, vb = pair & 2u;
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            const int py = y - L::ey(i), pz = z - L::ez(i);
+            const bool oy = py < 0 || py >= g.ny;
+            const bool oz = pz < 0 || pz >= g.nz;
+            const bool out = oy || oz;
+            const int pl = out ? edge_plane<Q, i>(oy, oz, p) : i;
+            const uint32_t off = out ? 0u : (uint32_t)link_offset<Q>(i, g);
+            const uint32_t sa = va ? c - off : c;
+            const uint32_t sb = vb ? c + 1u - off : c + 1u;
+            const T* base = fin + (size_t)pl * g.n;
+            if constexpr (S::kExact)
+                v[i] = make_float2(S::dec(S::ld(base + sa), L::w(i)), S::dec(S::ld(base + sb), L::w(i)));
+            else
+                v[i] = make_float2(S::raw(S::ld(base + sa)), S::raw(S::ld(base + sb)));
+        });
+        const unsigned bad = collide_pair<Q, S>(v, p.tau, p.cs) & pair;
+        if (bad) atomicOr(sl.diverged, 1);
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            T* dst = static_cast<T*>(pp.dst[i]);
+            if (pair == 3u) {
+                if constexpr (S::kExact)
+                    *reinterpret_cast<typename S::T2*>(dst + c) = S::enc2(v[i].x, v[i].y, L::w(i));
+                else
+                    *reinterpret_cast<typename S::T2*>(dst + c) = S::pack2(v[i].x, v[i].y);
+            } else {
+                if constexpr (S::kExact) {
+                    if (va) dst[c] = S::enc(v[i].x, L::w(i));
+                    if (vb) dst[c + 1u] = S::enc(v[i].y, L::w(i));
+                } else {
+                    const typename S::T2 h = S::pack2(v[i].x, v[i].y);
+                    if (va) dst[c] = h.x;
+                    if (vb) dst[c + 1u] = h.y;
+                }
+            }
+        });
+    }
+}
+
 template <int Q, class S>
 __global__ void __launch_bounds__(32 * kBulkRows) k_bulk_shell(const typename S::T* __restrict__ fin,
                                                                 typename S::T* __restrict__ fout,
@@ -588,13 +728,10 @@ __global__ void __launch_bounds__(32 * kBulkRows) k_bulk_shell(const typename S:
 // inlet/outlet planes) and the solid cells an outlet reads. Every link's source
 // address is formed with selects first and all loads issue together.
 template <int Q, class S>
-__global__ void __launch_bounds__(128) k_boundary_pull(const typename S::T* __restrict__ fin,
-                                                        typename S::T* __restrict__ fout, BoundaryList bl,
-                                                        uint32_t begin, uint32_t end, Geom g, StepParams p,
-                                                        int* __restrict__ diverged) {
+__device__ __forceinline__ void boundary_entry(const typename S::T* __restrict__ fin,
+                                               typename S::T* __restrict__ fout, const BoundaryList& bl, uint32_t e,
+                                               const Geom& g, const StepParams& p, int* __restrict__ diverged) {
     using L = Lattice<Q>;
-    const uint32_t e = begin + blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= end) return;
     const uint32_t c = __ldg(bl.cells + e);
     const unsigned long long lk = __ldg(bl.links + e);
     const unsigned cls = (unsigned)(lk >> kClassShift) & 7u;
@@ -647,6 +784,37 @@ __global__ void __launch_bounds__(128) k_boundary_pull(const typename S::T* __re
         constexpr int i = decltype(I)::value;
         store_pop_c<Q, S, i>(fout, g.n, c, f[i]);
     });
+}
+
+template <int Q, class S>
+__global__ void __launch_bounds__(128) k_boundary_pull(const typename S::T* __restrict__ fin,
+                                                        typename S::T* __restrict__ fout, BoundaryList bl,
+                                                        uint32_t begin, uint32_t end, Geom g, StepParams p,
+                                                        int* __restrict__ diverged) {
+    const uint32_t e = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= end) return;
+    boundary_entry<Q, S>(fin, fout, bl, e, g, p, diverged);
+}
+
+// The boundary-list entries of every lattice of a batch in one launch: a
+// thread takes one entry of the concatenated lists and finds its lattice by
+// binary search over the lattices' first entries.
+template <int Q, class S>
+__global__ void __launch_bounds__(128) k_boundary_pull_batch(const BatchLattice* __restrict__ lat, int nlat,
+                                                              unsigned long long total, int parity) {
+    const unsigned long long w = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= total) return;
+    int lo = 0, hi = nlat - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&lat[mid].bnd_first) <= w) lo = mid;
+        else hi = mid - 1;
+    }
+    const BatchLattice& L = lat[lo];
+    const int side = L.cur ^ parity;
+    boundary_entry<Q, S>(static_cast<const typename S::T*>(L.pop[side]),
+                         static_cast<typename S::T*>(const_cast<void*>(L.pop[side ^ 1])), L.bl,
+                         (uint32_t)(w - L.bnd_first), L.g, L.p, L.diverged);
 }
 
 // k_boundary_pull with the learned closure (16-bit offset storage): the same
@@ -895,6 +1063,56 @@ cudaError_t launch_boundary_pull_learned(int q, int storage, const void* fin, vo
                                          uint32_t begin, uint32_t end, const Geom& g, const StepParams& p,
                                          int* diverged, cudaStream_t s, const ClosureDev& cl) {
     FC_DISPATCH(q, storage, boundary_learned_t, fin, fout, bl, begin, end, g, p, diverged, s, cl);
+}
+
+template <int Q, class S>
+static cudaError_t bulk_batch_t(int rows, const BatchLattice* lat, int nlat, unsigned long long total, int parity,
+                                int grid, cudaStream_t s) {
+    if (total == 0) return cudaSuccess;
+    if (rows == 4)
+        k_bulk_pairs_batch<Q, S, 4><<<grid, dim3(32, 4), 0, s>>>(lat, nlat, total, parity);
+    else if (rows == 8)
+        k_bulk_pairs_batch<Q, S, 8><<<grid, dim3(32, 8), 0, s>>>(lat, nlat, total, parity);
+    else if (rows == 16)
+        k_bulk_pairs_batch<Q, S, 16><<<grid, dim3(32, 16), 0, s>>>(lat, nlat, total, parity);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+template <int Q, class S>
+static cudaError_t batch_resident_t(int rows, int* nb) {
+    if (rows == 4) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(nb, k_bulk_pairs_batch<Q, S, 4>, 128, 0);
+    if (rows == 8) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(nb, k_bulk_pairs_batch<Q, S, 8>, 256, 0);
+    if (rows == 16) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(nb, k_bulk_pairs_batch<Q, S, 16>, 512, 0);
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_bulk_batch(int q, int storage, int rows, const BatchLattice* lat, int nlat,
+                              unsigned long long total, int parity, int grid, cudaStream_t s) {
+    FC_DISPATCH(q, storage, bulk_batch_t, rows, lat, nlat, total, parity, grid, s);
+}
+
+template <int Q, class S>
+static cudaError_t boundary_batch_t(const BatchLattice* lat, int nlat, unsigned long long total, int parity,
+                                    cudaStream_t s) {
+    if (total == 0) return cudaSuccess;
+    k_boundary_pull_batch<Q, S><<<(unsigned)((total + 127) / 128), 128, 0, s>>>(lat, nlat, total, parity);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_boundary_batch(int q, int storage, const BatchLattice* lat, int nlat, unsigned long long total,
+                                  int parity, cudaStream_t s) {
+    FC_DISPATCH(q, storage, boundary_batch_t, lat, nlat, total, parity, s);
+}
+
+static cudaError_t batch_resident_dispatch(int q, int storage, int rows, int* nb) {
+    FC_DISPATCH(q, storage, batch_resident_t, rows, nb);
+}
+
+int bulk_batch_resident(int q, int storage, int rows) {
+    int nb = 0;
+    return batch_resident_dispatch(q, storage, rows, &nb) == cudaSuccess ? nb : 0;
 }
 
 cudaError_t launch_closure_probe(int q, int storage, const void* f, const Geom& g, const ClosureDev& cl, float* out,

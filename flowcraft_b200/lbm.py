@@ -150,6 +150,12 @@ SIGNATURES = {
     "fc_lbm_closure_probe": (ctypes.c_int, [_P, _FP, ctypes.POINTER(ctypes.c_uint8), _SZ]),
     "fc_lbm_wall_distance": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint8), _SZ]),
     "fc_lbm_closure_coverage": (ctypes.c_int, [_P, _U64P, _U64P]),
+    "fc_lbm_batch_create": (ctypes.c_int, [ctypes.POINTER(_P), _I32, ctypes.POINTER(_P)]),
+    "fc_lbm_batch_destroy": (None, [_P]),
+    "fc_lbm_batch_last_error": (ctypes.c_char_p, [_P]),
+    "fc_lbm_batch_step": (ctypes.c_int, [_P, _I32]),
+    "fc_lbm_batch_config": (ctypes.c_int, [_P, _I32, _I32]),
+    "fc_lbm_batch_tune": (ctypes.c_int, [_P, _I32, _I32P, _I32P, _FP]),
     "fc_lbm_closure_samples": (ctypes.c_int, [_P, ctypes.c_float, _P, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "fc_lbm_mlp_forward": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P, _P]),
     "fc_lbm_mlp_grad": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int64, _P, _P, _P, _P]),

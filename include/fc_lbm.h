@@ -310,6 +310,35 @@ FC_LBM_API int fc_lbm_mlp_grad(const float* params, const float* x, const float*
 FC_LBM_API int fc_lbm_mlp_adam(float* params, const float* grad, float* m, float* v, int32_t step, float lr,
                                float beta1, float beta2, float eps, void* stream);
 
+/* ---- Batches: many lattices stepped together (no reference counterpart) ----
+ * For sweeps such as a set of angles of attack: the members (initialized
+ * handles on one device, one lattice model and storage format, even nx, no
+ * learned closure) step together. Every step is one persistent bulk launch
+ * over a work-list of the tiles of all members and one launch over all their
+ * boundary lists; pairs of steps replay as one CUDA graph. Results are
+ * bit-identical to stepping every member with fc_lbm_step. The members keep
+ * their own state and API; they must outlive the batch and must not step on
+ * their own while a batch step is queued. */
+typedef struct fc_lbm_batch fc_lbm_batch;
+#define FC_LBM_BATCH_CANDIDATES 6
+FC_LBM_API int fc_lbm_batch_create(fc_lbm* const* members, int32_t count, fc_lbm_batch** out);
+FC_LBM_API void fc_lbm_batch_destroy(fc_lbm_batch* b);
+FC_LBM_API const char* fc_lbm_batch_last_error(const fc_lbm_batch* b);
+/* n steps of every member; asynchronous, ordered after and before the
+ * members' own streams. An odd n leaves the next call to rebuild its graph. */
+FC_LBM_API int fc_lbm_batch_step(fc_lbm_batch* b, int32_t n);
+/* The block shape of the persistent launch: rows in {4, 8, 16} (a block is 32
+ * x rows threads over 64 x rows cells), grid_mult in {1, 2} (resident blocks
+ * per SM times this). Default 8, 1. */
+FC_LBM_API int fc_lbm_batch_config(fc_lbm_batch* b, int32_t rows, int32_t grid_mult);
+/* Autotuner: times each of the FC_LBM_BATCH_CANDIDATES shapes (rows 4, 8, 16
+ * x grid_mult 1, 2, in that order) over `steps` (rounded up to even) real
+ * steps after 2 warm-up steps, and keeps the fastest. Every member advances
+ * by 6 x (steps + 2) steps (the candidates compute identical results).
+ * ms_per_step (may be NULL) receives each candidate's time. Blocking. */
+FC_LBM_API int fc_lbm_batch_tune(fc_lbm_batch* b, int32_t steps, int32_t* rows, int32_t* grid_mult,
+                                 float* ms_per_step);
+
 /* Statistics of a population set computed without allocating anything: no
  * cudaMalloc, cudaFree or allocating library call happens inside. This entry
  * point has no counterpart in the reference. It is meant for callers that
