@@ -827,6 +827,24 @@ int fc_lbm_wall_distance(fc_lbm* h, uint8_t* out, size_t cells) {
     return rc;
 }
 
+int fc_lbm_layer_copy(fc_lbm* h, int32_t z, int32_t next, void* buffer, int32_t to_buffer, void* stream) {
+    FC_RC(check_ready(h));
+    if (!buffer || z < 0 || z >= h->g.nz) return FC_LBM_ERR_INVALID_ARG;
+    DeviceGuard dg(h->device);
+    const size_t elem = h->storage == FC_STORAGE_FP32 ? 4 : 2;
+    const size_t width = (size_t)h->g.nxy * elem, pitch = h->g.n * elem;
+    char* pop = static_cast<char*>(h->pop[next ? 1 - h->cur : h->cur]) + (size_t)z * width;
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+    FC_RC(enter_stream(h, s));
+    // one strided copy: Q planes of one layer <-> Q contiguous rows
+    const cudaError_t e = to_buffer ? cudaMemcpy2DAsync(buffer, width, pop, pitch, width, (size_t)h->q,
+                                                        cudaMemcpyDeviceToDevice, s)
+                                    : cudaMemcpy2DAsync(pop, pitch, buffer, width, width, (size_t)h->q,
+                                                        cudaMemcpyDeviceToDevice, s);
+    FC_TRY(h, e, "layer copy");
+    return leave_stream(h, s);
+}
+
 int fc_lbm_probe_slice_health(fc_lbm* h, int32_t z, int32_t* diverged) {
     FC_RC(check_ready(h));
     if (!diverged) return FC_LBM_ERR_INVALID_ARG;

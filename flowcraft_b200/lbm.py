@@ -150,6 +150,7 @@ SIGNATURES = {
     "fc_lbm_closure_probe": (ctypes.c_int, [_P, _FP, ctypes.POINTER(ctypes.c_uint8), _SZ]),
     "fc_lbm_wall_distance": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint8), _SZ]),
     "fc_lbm_closure_coverage": (ctypes.c_int, [_P, _U64P, _U64P]),
+    "fc_lbm_layer_copy": (ctypes.c_int, [_P, _I32, _I32, _P, _I32, _P]),
     "fc_lbm_batch_create": (ctypes.c_int, [ctypes.POINTER(_P), _I32, ctypes.POINTER(_P)]),
     "fc_lbm_batch_destroy": (None, [_P]),
     "fc_lbm_batch_last_error": (ctypes.c_char_p, [_P]),
@@ -476,6 +477,13 @@ class LbmSolver:
         warps = (n + 63) // 64
         return {"cells_in_range": int(a.value), "cell_fraction": a.value / max(n, 1),
                 "warps_with_mlp": int(b.value), "warp_fraction": b.value / max(warps, 1)}
+
+    def LayerCopy(self, z: int, buffer_ptr: int, to_buffer: bool, next_set: bool = False, cmd=None) -> None:
+        """Packs (to_buffer) or unpacks z-layer `z` of the current (or, with
+        next_set, the in-progress step's output) population set to / from a
+        device buffer of Q*nx*ny elements."""
+        self._check(self._lib.fc_lbm_layer_copy(self._h, int(z), int(next_set), buffer_ptr, int(to_buffer),
+                                                _stream_ptr(cmd)), "LayerCopy")
 
     def WallDistance(self) -> np.ndarray:
         """The closure's wall-distance input, bytes in 1/16-cell steps."""

@@ -310,6 +310,15 @@ FC_LBM_API int fc_lbm_mlp_grad(const float* params, const float* x, const float*
 FC_LBM_API int fc_lbm_mlp_adam(float* params, const float* grad, float* m, float* v, int32_t step, float lr,
                                float beta1, float beta2, float eps, void* stream);
 
+/* Copies the Q populations of z-layer `z` between a population set and a
+ * contiguous DEVICE buffer of Q*nx*ny elements (storage format, plane i
+ * first): `next` = 0 is the current set, 1 the set the in-progress step
+ * writes (between fc_lbm_step_range and fc_lbm_advance_substep);
+ * `to_buffer` = 1 packs into the buffer, 0 unpacks from it. Asynchronous on
+ * `stream`. The halo exchange of a lattice split into z-slabs across GPUs
+ * (flowcraft_b200/shard.py) is built on it; no reference counterpart. */
+FC_LBM_API int fc_lbm_layer_copy(fc_lbm* h, int32_t z, int32_t next, void* buffer, int32_t to_buffer, void* stream);
+
 /* ---- Batches: many lattices stepped together (no reference counterpart) ----
  * For sweeps such as a set of angles of attack: the members (initialized
  * handles on one device, one lattice model and storage format, even nx, no
