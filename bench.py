@@ -59,7 +59,8 @@ CONFIGS = {
                     "Re=1e4 (tau=0.50173), Smagorinsky Cs=0.1"),
 }
 
-BYTES_PER_ELEM = {"fp32": 4, "fp16_offset": 2, "bf16_offset": 2, "fp16_learned": 2, "bf16_learned": 2}
+BYTES_PER_ELEM = {"fp32": 4, "fp16_offset": 2, "bf16_offset": 2, "fp16_learned": 2, "bf16_learned": 2,
+                  "fp32_aa": 4, "fp16_aa": 2, "bf16_aa": 2}
 # per-cell bytes beyond the populations: the closure's wall-distance byte
 EXTRA_BYTES = {"fp16_learned": 1, "bf16_learned": 1}
 CLOSURE_WEIGHTS = os.path.join(ROOT, "flowcraft_b200", "data", "closure_c4.json")
@@ -72,7 +73,8 @@ def parse_args(argv=None):
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="large")
-    ap.add_argument("--variants", default="fp16_learned,fp16_offset,fp32", help="first one is the headline")
+    ap.add_argument("--variants", default="fp16_learned,fp16_offset,fp32,fp16_aa,fp32_aa",
+                    help="first one is the headline; *_aa: one population set streamed in place")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -180,14 +182,21 @@ def build_geometry(cfg, device, z_lo=0, z_hi=None):
 def storage_of(variant):
     from flowcraft_b200 import Storage
     return {"fp32": Storage.FP32, "fp16_offset": Storage.FP16_OFFSET, "bf16_offset": Storage.BF16_OFFSET,
-            "fp16_learned": Storage.FP16_OFFSET, "bf16_learned": Storage.BF16_OFFSET}[variant]
+            "fp16_learned": Storage.FP16_OFFSET, "bf16_learned": Storage.BF16_OFFSET, "fp32_aa": Storage.FP32,
+            "fp16_aa": Storage.FP16_OFFSET, "bf16_aa": Storage.BF16_OFFSET}[variant]
+
+
+def streaming_of(variant):
+    """The *_aa variants keep one population set streamed in place."""
+    from flowcraft_b200 import Streaming
+    return Streaming.AA if variant.endswith("_aa") else Streaming.PINGPONG
 
 
 def make_solver(cfg, solid, sdf, variant, device_index):
     from flowcraft_b200 import LatticeModel, LbmSolver, Params, VoxelGrid
     s = LbmSolver()
     grid = VoxelGrid(cfg["nx"], cfg["ny"], cfg["nz"], solid=solid, signedDistance=sdf)
-    if not s.Init(device_index, grid, LatticeModel.D3Q19, storage_of(variant)):
+    if not s.Init(device_index, grid, LatticeModel.D3Q19, storage_of(variant), streaming_of(variant)):
         raise RuntimeError(s.LastError())
     s.Reset(Params(tau=tau_for(cfg), inletVelocity=cfg["u"], smagorinskyCs=cfg["cs"]), True)
     if variant.endswith("_learned"):

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/fc_lbm.h"
+#include "aa.cuh"
 #include "lattice.cuh"
 #include "lbm_internal.h"
 
@@ -34,8 +35,10 @@ struct fc_lbm {
     fc_params params{0.8f, 0.05f, 0, 1, 1, 0.12f};  // LbmSolver::Params defaults (LbmSolver.h:61-100)
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_own = nullptr, ev_foreign = nullptr, ev_sync = nullptr;
-    void* pop[2] = {nullptr, nullptr};
-    int cur = 0;
+    void* pop[2] = {nullptr, nullptr};  // AA streaming: one set, pop[1] == pop[0]
+    int cur = 0;                         // AA streaming: the next step's parity
+    void* d_aa_bz = nullptr;             // AA side buffers (lbm_internal.h AaSide)
+    float4* d_aa_outm = nullptr;
     uint8_t* d_solid = nullptr;
     float* d_sdf = nullptr;
     uint32_t* d_bulk_bits = nullptr;
@@ -172,6 +175,7 @@ fc::StepParams step_params(const fc_lbm* h) {
 
 void release(fc_lbm* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->pop[1] == h->pop[0]) h->pop[1] = nullptr;  // one in-place set
     dfree(h->pop[0]);
     dfree(h->pop[1]);
     dfree(h->d_solid);
@@ -188,6 +192,8 @@ void release(fc_lbm* h) {
     dfree(h->d_aero_result);
     dfree(h->d_closure);
     dfree(h->d_wall);
+    dfree(h->d_aa_bz);
+    dfree(h->d_aa_outm);
     h->closure_on = false;
     dfree(h->d_stage);
     if (h->h_stage) cudaFreeHost(h->h_stage);
@@ -319,9 +325,34 @@ int leave_stream(fc_lbm* h, cudaStream_t s) {
     return FC_LBM_OK;
 }
 
-// The two step kernels, with or without the learned closure.
+bool in_place(const fc_lbm* h) { return h->streaming == FC_STREAMING_AA; }
+
+// Where the current state's populations sit (aa.cuh PopLayout).
+int layout_of(const fc_lbm* h) { return in_place(h) ? fc::aa_layout(h->cur) : fc::kLayoutPlanes; }
+
+fc::AaSide aa_side(const fc_lbm* h) { return fc::AaSide{h->d_aa_bz, h->d_aa_outm, (size_t)h->g.ny * h->g.nz}; }
+
+fc::BoundaryList boundary_list(const fc_lbm* h) {
+    return fc::BoundaryList{h->d_cells, h->d_links, h->d_coef_off, h->d_coef};
+}
+
+// After a seed or a population load of an in-place lattice: the side
+// buffers from the new state.
+int aa_prime(fc_lbm* h) {
+    if (!in_place(h)) return FC_LBM_OK;
+    FC_TRY(h, fc::launch_aa_prime(h->q, h->storage, h->pop[0], boundary_list(h), (uint32_t)h->n_bnd, h->g, aa_side(h),
+                                  h->cur, h->stream),
+           "prime in-place side buffers");
+    h->launches += 2;
+    return FC_LBM_OK;
+}
+
+// The two step kernels, with or without the learned closure, ping-pong or in place.
 cudaError_t launch_bulk(fc_lbm* h, const fc::StepParams& p, const void* fin, void* fout, int z0, int zc,
                         cudaStream_t s, int* nl) {
+    if (in_place(h))
+        return fc::launch_bulk_aa(h->q, h->storage, h->pop[0], h->d_bulk_bits, h->g, p, z0, zc, h->d_diverged, s, nl,
+                                  h->cur, aa_side(h));
     if (h->closure_on)
         return fc::launch_bulk_pull_learned(h->q, h->storage, fin, fout, h->d_bulk_bits, h->g, p, z0, zc,
                                             h->d_diverged, s, nl, h->closure);
@@ -330,7 +361,10 @@ cudaError_t launch_bulk(fc_lbm* h, const fc::StepParams& p, const void* fin, voi
 
 cudaError_t launch_boundary(fc_lbm* h, const fc::StepParams& p, const void* fin, void* fout, uint32_t b, uint32_t e,
                             cudaStream_t s) {
-    const fc::BoundaryList bl{h->d_cells, h->d_links, h->d_coef_off, h->d_coef};
+    const fc::BoundaryList bl = boundary_list(h);
+    if (in_place(h))
+        return fc::launch_boundary_aa(h->q, h->storage, h->pop[0], bl, b, e, h->g, p, h->d_diverged, s, h->cur,
+                                      aa_side(h));
     if (h->closure_on)
         return fc::launch_boundary_pull_learned(h->q, h->storage, fin, fout, bl, b, e, h->g, p, h->d_diverged, s,
                                                 h->closure);
@@ -370,7 +404,7 @@ int field_to_host(fc_lbm* h, size_t cell0, size_t cells, float* out) {
     for (size_t done = 0; done < cells; done += chunk) {
         const size_t nc = std::min(chunk, cells - done);
         FC_TRY(h, fc::launch_field(h->q, h->storage, h->pop[h->cur], h->d_solid, h->d_sdf, h->g, cell0 + done, nc,
-                                   h->d_stage, h->stream),
+                                   h->d_stage, layout_of(h), h->stream),
                "field kernel");
         h->launches++;
         FC_TRY(h, cudaMemcpyAsync(h->h_stage, h->d_stage, nc * 4 * sizeof(float), cudaMemcpyDeviceToHost, h->stream),
@@ -425,8 +459,10 @@ int fc_lbm_init(fc_lbm* h, const fc_grid_desc* grid, int32_t model, const fc_opt
     if (opts) o = *opts;
     if (o.storage < FC_STORAGE_FP32 || o.storage > FC_STORAGE_BF16_OFFSET)
         return fail(h, FC_LBM_ERR_INVALID_ARG, "unknown storage format");
-    if (o.streaming != FC_STREAMING_PINGPONG)
-        return fail(h, FC_LBM_ERR_UNSUPPORTED, "only ping-pong streaming is available in this build");
+    if (o.streaming != FC_STREAMING_PINGPONG && o.streaming != FC_STREAMING_AA)
+        return fail(h, FC_LBM_ERR_INVALID_ARG, "unknown streaming mode");
+    if (o.streaming == FC_STREAMING_AA && (grid->nx % 2 != 0 || grid->nx < 4))
+        return fail(h, FC_LBM_ERR_UNSUPPORTED, "AA (in-place) streaming needs an even nx of at least 4");
     const size_t n = (size_t)grid->nx * (size_t)grid->ny * (size_t)grid->nz;
     if (n >= (size_t(1) << 32))
         return fail(h, FC_LBM_ERR_INVALID_ARG, "grid too large: at most 2^32-1 cells per lattice");
@@ -455,7 +491,8 @@ int fc_lbm_init(fc_lbm* h, const fc_grid_desc* grid, int32_t model, const fc_opt
     const size_t bits_bytes = (size_t)grid->ny * grid->nz * h->g.wpr * sizeof(uint32_t);
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
-        const size_t need = 2 * pop_bytes + n * (1 + (grid->signed_distance ? 4 : 0)) + bits_bytes + n /*flags*/;
+        const size_t sets = o.streaming == FC_STREAMING_AA ? 1 : 2;
+        const size_t need = sets * pop_bytes + n * (1 + (grid->signed_distance ? 4 : 0)) + bits_bytes + n /*flags*/;
         if (need > free_b) {
             char buf[256];
             std::snprintf(buf, sizeof(buf), "grid too large: %zu cells need %.2f GiB of device memory, %.2f GiB free",
@@ -473,7 +510,10 @@ int fc_lbm_init(fc_lbm* h, const fc_grid_desc* grid, int32_t model, const fc_opt
         FC_TRY(h, cudaMalloc(&h->d_stage, h->stage_floats * sizeof(float)), "alloc staging");
         FC_TRY(h, cudaMallocHost(&h->h_stage, h->stage_floats * sizeof(float)), "alloc pinned staging");
         FC_TRY(h, cudaMalloc(&h->pop[0], pop_bytes), "alloc populations");
-        FC_TRY(h, cudaMalloc(&h->pop[1], pop_bytes), "alloc populations");
+        if (in_place(h))
+            h->pop[1] = h->pop[0];  // readbacks use pop[cur] under either scheme
+        else
+            FC_TRY(h, cudaMalloc(&h->pop[1], pop_bytes), "alloc populations");
         FC_TRY(h, cudaMalloc(&h->d_solid, n), "alloc solid mask");
         if (grid->signed_distance) FC_TRY(h, cudaMalloc(&h->d_sdf, n * sizeof(float)), "alloc SDF");
         FC_TRY(h, cudaMalloc(&h->d_bulk_bits, bits_bytes), "alloc bulk mask");
@@ -490,6 +530,11 @@ int fc_lbm_init(fc_lbm* h, const fc_grid_desc* grid, int32_t model, const fc_opt
         FC_RC(upload(h, h->d_solid, grid->solid, n, dev));
         if (grid->signed_distance) FC_RC(upload(h, h->d_sdf, grid->signed_distance, n * sizeof(float), dev));
         FC_RC(build_boundary(h));
+        if (in_place(h)) {
+            FC_TRY(h, cudaMalloc(&h->d_aa_bz, std::max<size_t>(h->n_bz, 1) * elem), "alloc in-place link buffer");
+            FC_TRY(h, cudaMalloc(&h->d_aa_outm, 4 * (size_t)grid->ny * grid->nz * sizeof(float4)),
+                   "alloc in-place outlet buffer");
+        }
         h->solid_cpu.resize(n);
         if (dev) {
             FC_TRY(h, cudaMemcpy(h->solid_cpu.data(), grid->solid, n, cudaMemcpyDeviceToHost), "copy solid mask");
@@ -497,9 +542,12 @@ int fc_lbm_init(fc_lbm* h, const fc_grid_desc* grid, int32_t model, const fc_opt
             std::memcpy(h->solid_cpu.data(), grid->solid, n);
         }
         // A defined state before the first Reset: quiescent equilibrium.
-        FC_TRY(h, fc::launch_seed_uniform(h->q, h->storage, h->pop[0], h->g, 1.0f, 0.0f, 0.0f, 0.0f, h->stream),
+        h->cur = 0;
+        FC_TRY(h, fc::launch_seed_uniform(h->q, h->storage, h->pop[0], h->g, 1.0f, 0.0f, 0.0f, 0.0f, layout_of(h),
+                                          h->stream),
                "seed");
         h->launches++;
+        FC_RC(aa_prime(h));
         return wait_stream(h, kTransferTimeoutMs);
     };
     int rc = init_body();
@@ -529,10 +577,12 @@ int fc_lbm_reset(fc_lbm* h, const fc_params* params, int32_t seed_mid) {
         const float dev = 0.5f * (u * u - mid * mid);
         rho = 1.0f + 3.0f * dev;
     }
-    FC_TRY(h, fc::launch_seed_uniform(h->q, h->storage, h->pop[0], h->g, rho, ux, 0.0f, 0.0f, h->stream), "seed");
+    h->cur = 0;
+    FC_TRY(h, fc::launch_seed_uniform(h->q, h->storage, h->pop[0], h->g, rho, ux, 0.0f, 0.0f, layout_of(h), h->stream),
+           "seed");
     FC_TRY(h, cudaMemsetAsync(h->d_diverged, 0, sizeof(int), h->stream), "clear flag");
     h->launches++;
-    h->cur = 0;
+    FC_RC(aa_prime(h));
     h->steps_since_reset = 0;
     return FC_LBM_OK;
 }
@@ -542,6 +592,7 @@ int fc_lbm_reset_from_field(fc_lbm* h, const float* field, size_t count) {
     if (!field || count != h->g.n * 4)
         return fail(h, FC_LBM_ERR_INVALID_ARG, "field must hold exactly 4 floats per cell");
     DeviceGuard dg(h->device);
+    h->cur = 0;
     const size_t chunk = h->stage_floats / 4;
     for (size_t c0 = 0; c0 < h->g.n; c0 += chunk) {
         const size_t nc = std::min(chunk, h->g.n - c0);
@@ -549,12 +600,13 @@ int fc_lbm_reset_from_field(fc_lbm* h, const float* field, size_t count) {
         std::memcpy(h->h_stage, field + c0 * 4, nc * 4 * sizeof(float));
         FC_TRY(h, cudaMemcpyAsync(h->d_stage, h->h_stage, nc * 4 * sizeof(float), cudaMemcpyHostToDevice, h->stream),
                "field upload");
-        FC_TRY(h, fc::launch_seed_field(h->q, h->storage, h->pop[0], h->g, h->d_stage, h->d_solid, c0, nc, h->stream),
+        FC_TRY(h, fc::launch_seed_field(h->q, h->storage, h->pop[0], h->g, h->d_stage, h->d_solid, c0, nc,
+                                        layout_of(h), h->stream),
                "seed from field");
         h->launches++;
     }
     FC_TRY(h, cudaMemsetAsync(h->d_diverged, 0, sizeof(int), h->stream), "clear flag");
-    h->cur = 0;
+    FC_RC(aa_prime(h));
     h->steps_since_reset = 0;
     return wait_stream(h, kTransferTimeoutMs);
 }
@@ -624,7 +676,7 @@ int fc_lbm_readback_stats(fc_lbm* h, fc_stats* out) {
     if (!out) return FC_LBM_ERR_INVALID_ARG;
     DeviceGuard dg(h->device);
     FC_TRY(h, fc::launch_stats(h->q, h->storage, h->pop[h->cur], h->d_solid, h->d_sdf, h->g, h->d_stats_partials,
-                               h->stats_blocks, h->d_stats_result, h->stream),
+                               h->stats_blocks, h->d_stats_result, layout_of(h), h->stream),
            "stats kernel");
     h->launches += 2;
     FC_TRY(h, cudaMemcpyAsync(h->h_stage, h->d_stats_result, fc::kStatsSlots * sizeof(double), cudaMemcpyDeviceToHost,
@@ -664,7 +716,7 @@ int fc_lbm_aero_forces(fc_lbm* h, fc_aero_forces* out) {
     DeviceGuard dg(h->device);
     FC_TRY(h, fc::launch_aero(h->q, h->storage, h->pop[h->cur], h->d_solid, h->d_sdf, h->g, h->cell_size,
                               h->origin[0], h->origin[1], h->origin[2], h->d_aero_partials, h->stats_blocks,
-                              h->d_aero_result, h->stream),
+                              h->d_aero_result, layout_of(h), h->stream),
            "force kernel");
     h->launches += 2;
     FC_TRY(h, cudaMemcpyAsync(h->h_stage, h->d_aero_result, fc::kAeroResult * sizeof(double), cudaMemcpyDeviceToHost,
@@ -698,6 +750,7 @@ int fc_lbm_set_closure(fc_lbm* h, const fc_closure* c) {
     if (h->storage == FC_STORAGE_FP32)
         return fail(h, FC_LBM_ERR_UNSUPPORTED, "the learned closure runs on the FP16/BF16 offset storage formats");
     if (h->g.nx % 2 != 0) return fail(h, FC_LBM_ERR_UNSUPPORTED, "the learned closure needs an even nx");
+    if (in_place(h)) return fail(h, FC_LBM_ERR_UNSUPPORTED, "the learned closure runs with ping-pong streaming");
     if (!c->w1 || !c->b1 || !c->w2 || !c->b2 || !c->w3)
         return fail(h, FC_LBM_ERR_INVALID_ARG, "closure weights missing");
     bool ok = std::isfinite(c->b3) && std::isfinite(c->out_scale) && c->out_scale > 0.0f &&
@@ -752,6 +805,7 @@ int fc_lbm_set_closure(fc_lbm* h, const fc_closure* c) {
 int fc_lbm_closure_samples(fc_lbm* h, float filter_width, float* out, int64_t capacity, int64_t* count) {
     FC_RC(check_ready(h));
     if (!count || capacity < 0 || !std::isfinite(filter_width)) return FC_LBM_ERR_INVALID_ARG;
+    if (in_place(h)) return fail(h, FC_LBM_ERR_UNSUPPORTED, "closure samples need ping-pong streaming");
     DeviceGuard dg(h->device);
     FC_RC(wait_stream(h, kTransferTimeoutMs));  // every queued step first
     // the molecular relaxation time of the 2x coarser lattice (nu halves)
@@ -830,6 +884,7 @@ int fc_lbm_wall_distance(fc_lbm* h, uint8_t* out, size_t cells) {
 int fc_lbm_layer_copy(fc_lbm* h, int32_t z, int32_t next, void* buffer, int32_t to_buffer, void* stream) {
     FC_RC(check_ready(h));
     if (!buffer || z < 0 || z >= h->g.nz) return FC_LBM_ERR_INVALID_ARG;
+    if (in_place(h)) return fail(h, FC_LBM_ERR_UNSUPPORTED, "layer copies need ping-pong streaming");
     DeviceGuard dg(h->device);
     const size_t elem = h->storage == FC_STORAGE_FP32 ? 4 : 2;
     const size_t width = (size_t)h->g.nxy * elem, pitch = h->g.n * elem;
@@ -857,7 +912,7 @@ int fc_lbm_probe_slice_health(fc_lbm* h, int32_t z, int32_t* diverged) {
     for (size_t done = 0; done < layer; done += chunk) {
         const size_t nc = std::min(chunk, layer - done);
         FC_TRY(h, fc::launch_field(h->q, h->storage, h->pop[h->cur], h->d_solid, h->d_sdf, h->g, c0 + done, nc,
-                                   h->d_stage, h->stream),
+                                   h->d_stage, layout_of(h), h->stream),
                "field kernel");
         h->launches++;
         FC_TRY(h, cudaMemcpyAsync(h->h_stage, h->d_stage, nc * 4 * sizeof(float), cudaMemcpyDeviceToHost, h->stream),
@@ -1011,7 +1066,7 @@ int fc_lbm_save_populations(fc_lbm* h, float* out, size_t count) {
     for (size_t c0 = 0; c0 < h->g.n; c0 += chunk) {
         const size_t nc = std::min(chunk, h->g.n - c0);
         FC_TRY(h, fc::launch_pops_out(h->q, h->storage, h->pop[h->cur], h->d_solid, solid_w, h->g, c0, nc, h->d_stage,
-                                      h->stream),
+                                      layout_of(h), h->stream),
                "population readout");
         h->launches++;
         FC_TRY(h, cudaMemcpyAsync(h->h_stage, h->d_stage, nc * h->q * sizeof(float), cudaMemcpyDeviceToHost, h->stream),
@@ -1036,10 +1091,12 @@ int fc_lbm_load_populations(fc_lbm* h, const float* in, size_t count) {
             std::memcpy(h->h_stage + (size_t)i * nc, in + (size_t)i * h->g.n + c0, nc * sizeof(float));
         FC_TRY(h, cudaMemcpyAsync(h->d_stage, h->h_stage, nc * h->q * sizeof(float), cudaMemcpyHostToDevice, h->stream),
                "population upload");
-        FC_TRY(h, fc::launch_pops_in(h->q, h->storage, h->pop[h->cur], h->g, c0, nc, h->d_stage, h->stream),
+        FC_TRY(h, fc::launch_pops_in(h->q, h->storage, h->pop[h->cur], h->g, c0, nc, h->d_stage, layout_of(h),
+                                     h->stream),
                "population write");
         h->launches++;
     }
+    FC_RC(aa_prime(h));
     // The loaded state is a post-step state: solid cells hold what was given.
     h->steps_since_reset = 0;
     return wait_stream(h, kTransferTimeoutMs);
@@ -1253,7 +1310,7 @@ int fc_lbm_batch_create(fc_lbm* const* members, int32_t count, fc_lbm_batch** ou
         fc_lbm* h = members[k];
         if (!h || !h->valid) return FC_LBM_ERR_NOT_INITIALIZED;
         if (h->device != h0->device || h->q != h0->q || h->storage != h0->storage) return FC_LBM_ERR_INVALID_ARG;
-        if (h->g.nx % 2 != 0 || h->closure_on) return FC_LBM_ERR_UNSUPPORTED;
+        if (h->g.nx % 2 != 0 || h->closure_on || in_place(h)) return FC_LBM_ERR_UNSUPPORTED;
         for (int j = 0; j < k; ++j)
             if (members[j] == h) return FC_LBM_ERR_INVALID_ARG;
     }

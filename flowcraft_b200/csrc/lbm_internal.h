@@ -153,6 +153,28 @@ cudaError_t launch_boundary_batch(int q, int storage, const BatchLattice* lat, i
 // Blocks of the batch kernel resident per SM (occupancy), or 0.
 int bulk_batch_resident(int q, int storage, int rows);
 
+// Side buffers of a lattice streamed in place (lbm_step_aa.cu): `bz` holds
+// one stored population per Bouzidi coefficient slot (the far-side partner
+// f*_i(c) of that link from the previous step), `outm` 2 parities x 2
+// columns x `rows` (= ny * nz) moments (rho, ux, uy, uz) of the cells at
+// x = 1 and x = nx-2 for the outlets.
+struct AaSide {
+    void* bz;
+    float4* outm;
+    size_t rows;
+};
+// One in-place step's bulk and boundary kernels; `odd` is the step's parity
+// (0: reads the kLayoutAAEven state, 1: kLayoutAAOdd). Even nx >= 4 only.
+cudaError_t launch_bulk_aa(int q, int storage, void* f, const uint32_t* bulk_bits, const Geom& g, const StepParams& p,
+                           int z0, int zc, int* diverged, cudaStream_t s, int* launched, int odd, const AaSide& sd);
+cudaError_t launch_boundary_aa(int q, int storage, void* f, const BoundaryList& bl, uint32_t begin, uint32_t end,
+                               const Geom& g, const StepParams& p, int* diverged, cudaStream_t s, int odd,
+                               const AaSide& sd);
+// Fills the side buffers from the state a step of parity `par` reads (after a
+// seed or a population load); `count` = boundary-list length.
+cudaError_t launch_aa_prime(int q, int storage, const void* f, const BoundaryList& bl, uint32_t count, const Geom& g,
+                            const AaSide& sd, int par, cudaStream_t s);
+
 cudaError_t launch_bulk_pull(int q, int storage, const void* fin, void* fout, const uint32_t* bulk_bits,
                              const Geom& g, const StepParams& p, int z0, int zc, int* diverged, cudaStream_t s,
                              int* launched);
@@ -163,24 +185,27 @@ cudaError_t launch_boundary_pull(int q, int storage, const void* fin, void* fout
                                  uint32_t begin, uint32_t end, const Geom& g, const StepParams& p, int* diverged,
                                  cudaStream_t s);
 
+// `layout` (every launcher that reads or writes a whole state): where the
+// populations sit between steps, a PopLayout of aa.cuh: 0 plane-major
+// (ping-pong), 1 / 2 one set streamed in place before an even / odd step.
 cudaError_t launch_seed_uniform(int q, int storage, void* f, const Geom& g, float rho, float ux, float uy, float uz,
-                                cudaStream_t s);
+                                int layout, cudaStream_t s);
 cudaError_t launch_seed_field(int q, int storage, void* f, const Geom& g, const float* field, const uint8_t* solid,
-                              size_t cell0, size_t cells, cudaStream_t s);
+                              size_t cell0, size_t cells, int layout, cudaStream_t s);
 
 cudaError_t launch_field(int q, int storage, const void* f, const uint8_t* solid, const float* sdf, const Geom& g,
-                         size_t cell0, size_t cells, float* out, cudaStream_t s);
+                         size_t cell0, size_t cells, float* out, int layout, cudaStream_t s);
 cudaError_t launch_pops_out(int q, int storage, const void* f, const uint8_t* solid, int solid_is_weight,
-                            const Geom& g, size_t cell0, size_t cells, float* out, cudaStream_t s);
+                            const Geom& g, size_t cell0, size_t cells, float* out, int layout, cudaStream_t s);
 cudaError_t launch_pops_in(int q, int storage, void* f, const Geom& g, size_t cell0, size_t cells,
-                           const float* in, cudaStream_t s);
+                           const float* in, int layout, cudaStream_t s);
 
 // Stats: `partials` holds stats_partial_doubles() doubles per block of
 // stats_blocks(); `result` receives kStatsSlots doubles.
 constexpr int kStatsSlots = 12;
 int stats_blocks(const Geom& g);
 cudaError_t launch_stats(int q, int storage, const void* f, const uint8_t* solid, const float* sdf, const Geom& g,
-                         double* partials, int blocks, double* result, cudaStream_t s);
+                         double* partials, int blocks, double* result, int layout, cudaStream_t s);
 
 // Aerodynamic force integral (FieldOverlay::ComputeAerodynamicForces). The
 // partials take stats_blocks(g) * kAeroSlots doubles; `result` receives
@@ -191,7 +216,7 @@ constexpr int kAeroSlots = 20;
 constexpr int kAeroResult = 16;
 cudaError_t launch_aero(int q, int storage, const void* f, const uint8_t* solid, const float* sdf, const Geom& g,
                         float cell_size, float ox, float oy, float oz, double* partials, int blocks, double* result,
-                        cudaStream_t s);
+                        int layout, cudaStream_t s);
 
 // Setup (geometry classification and boundary-list construction).
 // counts[0] += flagged (boundary-list) cells, counts[1] += bulk cells.

@@ -12,6 +12,7 @@
 // cell update.
 #include <mutex>
 
+#include "aa.cuh"
 #include "collide.cuh"
 #include "fc_lbm.h"
 #include "lbm_internal.h"
@@ -24,15 +25,22 @@ __device__ __forceinline__ bool inb(const Geom& g, int x, int y, int z) {
 }
 __device__ __forceinline__ size_t cidx(const Geom& g, int x, int y, int z) { return ((size_t)z * g.ny + y) * g.nx + x; }
 
+// Post-collision population P of cell c = (x, y, z) under `layout` (aa.cuh).
+template <int Q, class S, int P>
+__device__ __forceinline__ float load_at(const typename S::T* __restrict__ f, size_t c, int x, int y, int z,
+                                         const Geom& g, int layout) {
+    return S::dec(S::ld(f + pop_slot<Q, P>(c, x, y, z, g, layout)), Lattice<Q>::w(P));
+}
+
 // InterpolatedBounceBack for fluid node a (cell ca) whose direction-i
 // upstream neighbour s (cell cs) is solid (LbmReference.cpp:100-122).
 template <int Q, class S, int I>
 __device__ float bounce_rt(const typename S::T* __restrict__ f, const uint8_t* __restrict__ solid,
                            const float* __restrict__ sdf, const Geom& g, int ax, int ay, int az, size_t ca,
-                           size_t cs) {
+                           size_t cs, int layout) {
     using L = Lattice<Q>;
     constexpr int op = L::opp(I);
-    const float plain = load_pop_c<Q, S, op>(f, g.n, ca);
+    const float plain = load_at<Q, S, op>(f, ca, ax, ay, az, g, layout);
     if (!sdf) return plain;
     const float phi_f = sdf[ca], phi_s = sdf[cs];
     if (!isfinite(phi_f) || !isfinite(phi_s)) return plain;
@@ -43,15 +51,16 @@ __device__ float bounce_rt(const typename S::T* __restrict__ f, const uint8_t* _
     if (q < 0.5f) {
         const int fx = ax + L::ex(I), fy = ay + L::ey(I), fz = az + L::ez(I);
         if (!inb(g, fx, fy, fz) || solid[cidx(g, fx, fy, fz)]) return plain;
-        return 2.0f * q * plain + (1.0f - 2.0f * q) * load_pop_c<Q, S, op>(f, g.n, cidx(g, fx, fy, fz));
+        return 2.0f * q * plain + (1.0f - 2.0f * q) * load_at<Q, S, op>(f, cidx(g, fx, fy, fz), fx, fy, fz, g, layout);
     }
     const float inv = 1.0f / (2.0f * q);
-    return inv * plain + (1.0f - inv) * load_pop_c<Q, S, I>(f, g.n, ca);
+    return inv * plain + (1.0f - inv) * load_at<Q, S, I>(f, ca, ax, ay, az, g, layout);
 }
 
 template <int Q, class S>
 __device__ float4 solid_force(const typename S::T* __restrict__ f, const uint8_t* __restrict__ solid,
-                              const float* __restrict__ sdf, const Geom& g, int x, int y, int z, size_t c) {
+                              const float* __restrict__ sdf, const Geom& g, int x, int y, int z, size_t c,
+                              int layout) {
     using L = Lattice<Q>;
     float fx = 0.0f, fy = 0.0f, fz = 0.0f, ws = 0.0f;
     static_for<1, Q>([&](auto I) {
@@ -61,8 +70,8 @@ __device__ float4 solid_force(const typename S::T* __restrict__ f, const uint8_t
         if (!inb(g, ax, ay, az)) return;
         const size_t ca = cidx(g, ax, ay, az);
         if (solid[ca]) return;
-        const float plain = load_pop_c<Q, S, L::opp(i)>(f, g.n, ca);
-        const float bounced = bounce_rt<Q, S, i>(f, solid, sdf, g, ax, ay, az, ca, c);
+        const float plain = load_at<Q, S, L::opp(i)>(f, ca, ax, ay, az, g, layout);
+        const float bounced = bounce_rt<Q, S, i>(f, solid, sdf, g, ax, ay, az, ca, c, layout);
         const float dp = (plain + bounced) - 2.0f * L::w(i);
         if constexpr (X > 0) fx = fx - dp;
         if constexpr (X < 0) fx = fx + dp;
@@ -78,11 +87,12 @@ __device__ float4 solid_force(const typename S::T* __restrict__ f, const uint8_t
 }
 
 template <int Q, class S>
-__device__ __forceinline__ float4 fluid_moments(const typename S::T* __restrict__ f, const Geom& g, size_t c) {
+__device__ __forceinline__ float4 fluid_moments(const typename S::T* __restrict__ f, const Geom& g, size_t c, int x,
+                                                int y, int z, int layout) {
     float p[Q];
     static_for<0, Q>([&](auto I) {
         constexpr int i = decltype(I)::value;
-        p[i] = load_pop_c<Q, S, i>(f, g.n, c);
+        p[i] = load_at<Q, S, i>(f, c, x, y, z, g, layout);
     });
     float rho, ux, uy, uz;
     moments<Q>(p, rho, ux, uy, uz);
@@ -92,7 +102,7 @@ __device__ __forceinline__ float4 fluid_moments(const typename S::T* __restrict_
 template <int Q, class S>
 __global__ void __launch_bounds__(256) k_field(const typename S::T* __restrict__ f, const uint8_t* __restrict__ solid,
                                                 const float* __restrict__ sdf, Geom g, size_t cell0, size_t cells,
-                                                float4* __restrict__ out) {
+                                                float4* __restrict__ out, int layout) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= cells) return;
     const size_t c = cell0 + k;
@@ -100,31 +110,41 @@ __global__ void __launch_bounds__(256) k_field(const typename S::T* __restrict__
     const size_t rem = c - (size_t)z * g.nxy;
     const int y = (int)(rem / g.nx);
     const int x = (int)(rem - (size_t)y * g.nx);
-    out[k] = solid[c] ? solid_force<Q, S>(f, solid, sdf, g, x, y, z, c) : fluid_moments<Q, S>(f, g, c);
+    out[k] = solid[c] ? solid_force<Q, S>(f, solid, sdf, g, x, y, z, c, layout)
+                      : fluid_moments<Q, S>(f, g, c, x, y, z, layout);
 }
 
 template <int Q, class S>
 __global__ void k_pops_out(const typename S::T* __restrict__ f, const uint8_t* __restrict__ solid,
-                           int solid_is_weight, Geom g, size_t cell0, size_t cells, float* __restrict__ out) {
+                           int solid_is_weight, Geom g, size_t cell0, size_t cells, float* __restrict__ out,
+                           int layout) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= cells) return;
     const size_t c = cell0 + k;
+    const int z = (int)(c / (size_t)g.nxy);
+    const size_t rem = c - (size_t)z * g.nxy;
+    const int y = (int)(rem / g.nx);
+    const int x = (int)(rem - (size_t)y * g.nx);
     const bool sw = solid_is_weight && solid[c];
     static_for<0, Q>([&](auto I) {
         constexpr int i = decltype(I)::value;
-        out[(size_t)i * cells + k] = sw ? Lattice<Q>::w(i) : load_pop_c<Q, S, i>(f, g.n, c);
+        out[(size_t)i * cells + k] = sw ? Lattice<Q>::w(i) : load_at<Q, S, i>(f, c, x, y, z, g, layout);
     });
 }
 
 template <int Q, class S>
 __global__ void k_pops_in(typename S::T* __restrict__ f, Geom g, size_t cell0, size_t cells,
-                          const float* __restrict__ in) {
+                          const float* __restrict__ in, int layout) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= cells) return;
     const size_t c = cell0 + k;
+    const int z = (int)(c / (size_t)g.nxy);
+    const size_t rem = c - (size_t)z * g.nxy;
+    const int y = (int)(rem / g.nx);
+    const int x = (int)(rem - (size_t)y * g.nx);
     static_for<0, Q>([&](auto I) {
         constexpr int i = decltype(I)::value;
-        store_pop_c<Q, S, i>(f, g.n, c, in[(size_t)i * cells + k]);
+        f[pop_slot<Q, i>(c, x, y, z, g, layout)] = S::enc(in[(size_t)i * cells + k], Lattice<Q>::w(i));
     });
 }
 
@@ -195,15 +215,15 @@ template <int Q, class S>
 __global__ void __launch_bounds__(kStatsThreads) k_stats(const typename S::T* __restrict__ f,
                                                          const uint8_t* __restrict__ solid,
                                                          const float* __restrict__ sdf, Geom g,
-                                                         double* __restrict__ partials) {
+                                                         double* __restrict__ partials, int layout) {
     StatAcc acc;
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < g.n; c += (size_t)gridDim.x * blockDim.x) {
+        const int z = (int)(c / (size_t)g.nxy);
+        const size_t rem = c - (size_t)z * g.nxy;
+        const int y = (int)(rem / g.nx);
+        const int x = (int)(rem - (size_t)y * g.nx);
         if (solid[c]) {
-            const int z = (int)(c / (size_t)g.nxy);
-            const size_t rem = c - (size_t)z * g.nxy;
-            const int y = (int)(rem / g.nx);
-            const int x = (int)(rem - (size_t)y * g.nx);
-            const float4 v = solid_force<Q, S>(f, solid, sdf, g, x, y, z, c);
+            const float4 v = solid_force<Q, S>(f, solid, sdf, g, x, y, z, c, layout);
             if (isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(v.w)) {
                 acc.fx += (double)v.y;
                 acc.fy += (double)v.z;
@@ -212,7 +232,7 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats(const typename S::T* __
             }
             continue;
         }
-        const float4 m = fluid_moments<Q, S>(f, g, c);
+        const float4 m = fluid_moments<Q, S>(f, g, c, x, y, z, layout);
         if (!isfinite(m.x) || !isfinite(m.y) || !isfinite(m.z) || !isfinite(m.w)) {
             acc.nan = 1;
             continue;
@@ -296,7 +316,8 @@ template <int Q, class S>
 __global__ void __launch_bounds__(kStatsThreads) k_aero(const typename S::T* __restrict__ f,
                                                         const uint8_t* __restrict__ solid,
                                                         const float* __restrict__ sdf, Geom g, float cs, float ox,
-                                                        float oy, float oz, double* __restrict__ partials) {
+                                                        float oy, float oz, double* __restrict__ partials,
+                                                        int layout) {
     double a[kAeroSlots];
     aero_init(a);
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < g.n; c += (size_t)gridDim.x * blockDim.x) {
@@ -314,7 +335,7 @@ __global__ void __launch_bounds__(kStatsThreads) k_aero(const typename S::T* __r
         a[kAgx + 2] += (double)pz;
         a[kAcount] += 1.0;
         a[kAmaxz] = fmax(a[kAmaxz], (double)z);
-        const float4 v = solid_force<Q, S>(f, solid, sdf, g, x, y, z, c);
+        const float4 v = solid_force<Q, S>(f, solid, sdf, g, x, y, z, c, layout);
         if (!isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z) || !isfinite(v.w)) {
             a[kAnan] = 1.0;
             continue;
@@ -422,33 +443,34 @@ int stats_blocks(const Geom& g) {
 
 template <int Q, class S>
 static cudaError_t field_t(const void* f, const uint8_t* solid, const float* sdf, const Geom& g, size_t cell0,
-                           size_t cells, float* out, cudaStream_t s) {
+                           size_t cells, float* out, int layout, cudaStream_t s) {
     if (cells == 0) return cudaSuccess;
     k_field<Q, S><<<(unsigned)((cells + 255) / 256), 256, 0, s>>>((const typename S::T*)f, solid, sdf, g, cell0, cells,
-                                                                  (float4*)out);
+                                                                  (float4*)out, layout);
     return cudaGetLastError();
 }
 
 template <int Q, class S>
 static cudaError_t pops_out_t(const void* f, const uint8_t* solid, int sw, const Geom& g, size_t cell0, size_t cells,
-                              float* out, cudaStream_t s) {
+                              float* out, int layout, cudaStream_t s) {
     if (cells == 0) return cudaSuccess;
     k_pops_out<Q, S><<<(unsigned)((cells + 255) / 256), 256, 0, s>>>((const typename S::T*)f, solid, sw, g, cell0,
-                                                                     cells, out);
+                                                                     cells, out, layout);
     return cudaGetLastError();
 }
 
 template <int Q, class S>
-static cudaError_t pops_in_t(void* f, const Geom& g, size_t cell0, size_t cells, const float* in, cudaStream_t s) {
+static cudaError_t pops_in_t(void* f, const Geom& g, size_t cell0, size_t cells, const float* in, int layout,
+                             cudaStream_t s) {
     if (cells == 0) return cudaSuccess;
-    k_pops_in<Q, S><<<(unsigned)((cells + 255) / 256), 256, 0, s>>>((typename S::T*)f, g, cell0, cells, in);
+    k_pops_in<Q, S><<<(unsigned)((cells + 255) / 256), 256, 0, s>>>((typename S::T*)f, g, cell0, cells, in, layout);
     return cudaGetLastError();
 }
 
 template <int Q, class S>
 static cudaError_t stats_t(const void* f, const uint8_t* solid, const float* sdf, const Geom& g, double* partials,
-                           int blocks, double* result, cudaStream_t s) {
-    k_stats<Q, S><<<blocks, kStatsThreads, 0, s>>>((const typename S::T*)f, solid, sdf, g, partials);
+                           int blocks, double* result, int layout, cudaStream_t s) {
+    k_stats<Q, S><<<blocks, kStatsThreads, 0, s>>>((const typename S::T*)f, solid, sdf, g, partials, layout);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_stats_final<<<1, kStatsThreads, 0, s>>>(partials, blocks, result);
@@ -470,29 +492,31 @@ static cudaError_t stats_t(const void* f, const uint8_t* solid, const float* sdf
     } while (0)
 
 cudaError_t launch_field(int q, int storage, const void* f, const uint8_t* solid, const float* sdf, const Geom& g,
-                         size_t cell0, size_t cells, float* out, cudaStream_t s) {
-    FC_DISPATCH(q, storage, field_t, f, solid, sdf, g, cell0, cells, out, s);
+                         size_t cell0, size_t cells, float* out, int layout, cudaStream_t s) {
+    FC_DISPATCH(q, storage, field_t, f, solid, sdf, g, cell0, cells, out, layout, s);
 }
 
 cudaError_t launch_pops_out(int q, int storage, const void* f, const uint8_t* solid, int solid_is_weight,
-                            const Geom& g, size_t cell0, size_t cells, float* out, cudaStream_t s) {
-    FC_DISPATCH(q, storage, pops_out_t, f, solid, solid_is_weight, g, cell0, cells, out, s);
+                            const Geom& g, size_t cell0, size_t cells, float* out, int layout, cudaStream_t s) {
+    FC_DISPATCH(q, storage, pops_out_t, f, solid, solid_is_weight, g, cell0, cells, out, layout, s);
 }
 
 cudaError_t launch_pops_in(int q, int storage, void* f, const Geom& g, size_t cell0, size_t cells, const float* in,
-                           cudaStream_t s) {
-    FC_DISPATCH(q, storage, pops_in_t, f, g, cell0, cells, in, s);
+                           int layout, cudaStream_t s) {
+    FC_DISPATCH(q, storage, pops_in_t, f, g, cell0, cells, in, layout, s);
 }
 
 cudaError_t launch_stats(int q, int storage, const void* f, const uint8_t* solid, const float* sdf, const Geom& g,
-                         double* partials, int blocks, double* result, cudaStream_t s) {
-    FC_DISPATCH(q, storage, stats_t, f, solid, sdf, g, partials, blocks, result, s);
+                         double* partials, int blocks, double* result, int layout, cudaStream_t s) {
+    FC_DISPATCH(q, storage, stats_t, f, solid, sdf, g, partials, blocks, result, layout, s);
 }
 
 template <int Q, class S>
 static cudaError_t aero_t(const void* f, const uint8_t* solid, const float* sdf, const Geom& g, float cs, float ox,
-                          float oy, float oz, double* partials, int blocks, double* result, cudaStream_t s) {
-    k_aero<Q, S><<<blocks, kStatsThreads, 0, s>>>((const typename S::T*)f, solid, sdf, g, cs, ox, oy, oz, partials);
+                          float oy, float oz, double* partials, int blocks, double* result, int layout,
+                          cudaStream_t s) {
+    k_aero<Q, S><<<blocks, kStatsThreads, 0, s>>>((const typename S::T*)f, solid, sdf, g, cs, ox, oy, oz, partials,
+                                                  layout);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_aero_final<<<1, kStatsThreads, 0, s>>>(partials, blocks, solid, g, cs, ox, oy, oz, result);
@@ -501,8 +525,8 @@ static cudaError_t aero_t(const void* f, const uint8_t* solid, const float* sdf,
 
 cudaError_t launch_aero(int q, int storage, const void* f, const uint8_t* solid, const float* sdf, const Geom& g,
                         float cell_size, float ox, float oy, float oz, double* partials, int blocks, double* result,
-                        cudaStream_t s) {
-    FC_DISPATCH(q, storage, aero_t, f, solid, sdf, g, cell_size, ox, oy, oz, partials, blocks, result, s);
+                        int layout, cudaStream_t s) {
+    FC_DISPATCH(q, storage, aero_t, f, solid, sdf, g, cell_size, ox, oy, oz, partials, blocks, result, layout, s);
 }
 
 }  // namespace fc
@@ -564,6 +588,6 @@ extern "C" FC_LBM_API int fc_lbm_stats_noalloc(const void* populations, const ui
     const int blocks = (int)((n + kNoAllocCellsPerBlock - 1) / kNoAllocCellsPerBlock);
     const int q = model == FC_LATTICE_D3Q19 ? 19 : 15;
     const cudaError_t e = fc::launch_stats(q, storage, populations, solid, signed_distance, g, scratch, blocks,
-                                           out_slots, static_cast<cudaStream_t>(stream));
+                                           out_slots, fc::kLayoutPlanes, static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? FC_LBM_OK : FC_LBM_ERR_CUDA;
 }

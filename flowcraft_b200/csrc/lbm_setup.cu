@@ -15,6 +15,7 @@
 #include <cub/device/device_select.cuh>
 #include <thrust/iterator/counting_iterator.h>
 
+#include "aa.cuh"
 #include "collide.cuh"
 #include "lbm_internal.h"
 #include "storage.cuh"
@@ -155,21 +156,40 @@ __global__ void k_z_offsets(const uint32_t* __restrict__ cells, size_t count, Ge
     z_begin[z] = (uint32_t)lo;
 }
 
+// Writes populations e[] of cell c where `layout` keeps them (aa.cuh).
 template <int Q, class S>
-__global__ void k_seed_uniform(typename S::T* __restrict__ f, size_t n, float rho, float ux, float uy, float uz) {
+__device__ __forceinline__ void seed_cell(typename S::T* __restrict__ f, const Geom& g, size_t c, const float (&e)[Q],
+                                          int layout) {
+    const int z = (int)(c / (size_t)g.nxy);
+    const size_t rem = c - (size_t)z * g.nxy;
+    const int y = (int)(rem / g.nx);
+    const int x = (int)(rem - (size_t)y * g.nx);
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        f[pop_slot<Q, i>(c, x, y, z, g, layout)] = S::enc(e[i], Lattice<Q>::w(i));
+    });
+}
+
+template <int Q, class S>
+__global__ void k_seed_uniform(typename S::T* __restrict__ f, Geom g, float rho, float ux, float uy, float uz,
+                               int layout) {
     float e[Q];
     equilibrium_all<Q>(rho, ux, uy, uz, e);
-    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
-        static_for<0, Q>([&](auto I) {
-            constexpr int i = decltype(I)::value;
-            store_pop_c<Q, S, i>(f, n, c, e[i]);
-        });
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < g.n; c += (size_t)gridDim.x * blockDim.x) {
+        if (layout == kLayoutPlanes) {
+            static_for<0, Q>([&](auto I) {
+                constexpr int i = decltype(I)::value;
+                store_pop_c<Q, S, i>(f, g.n, c, e[i]);
+            });
+        } else {
+            seed_cell<Q, S>(f, g, c, e, layout);
+        }
     }
 }
 
 template <int Q, class S>
-__global__ void k_seed_field(typename S::T* __restrict__ f, size_t n, const float4* __restrict__ field,
-                             const uint8_t* __restrict__ solid, size_t cell0, size_t cells) {
+__global__ void k_seed_field(typename S::T* __restrict__ f, Geom g, const float4* __restrict__ field,
+                             const uint8_t* __restrict__ solid, size_t cell0, size_t cells, int layout) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= cells) return;
     const size_t c = cell0 + k;
@@ -177,25 +197,24 @@ __global__ void k_seed_field(typename S::T* __restrict__ f, size_t n, const floa
     if (solid[c]) v = make_float4(1.0f, 0.0f, 0.0f, 0.0f);  // LbmReference.cpp:231-234
     float e[Q];
     equilibrium_all<Q>(v.x, v.y, v.z, v.w, e);
-    static_for<0, Q>([&](auto I) {
-        constexpr int i = decltype(I)::value;
-        store_pop_c<Q, S, i>(f, n, c, e[i]);
-    });
+    seed_cell<Q, S>(f, g, c, e, layout);
 }
 
 template <int Q, class S>
-static cudaError_t seed_uniform_t(void* f, const Geom& g, float rho, float ux, float uy, float uz, cudaStream_t s) {
+static cudaError_t seed_uniform_t(void* f, const Geom& g, float rho, float ux, float uy, float uz, int layout,
+                                  cudaStream_t s) {
     const unsigned blocks = 148 * 8;
-    k_seed_uniform<Q, S><<<blocks, 256, 0, s>>>((typename S::T*)f, g.n, rho, ux, uy, uz);
+    k_seed_uniform<Q, S><<<blocks, 256, 0, s>>>((typename S::T*)f, g, rho, ux, uy, uz, layout);
     return cudaGetLastError();
 }
 
 template <int Q, class S>
 static cudaError_t seed_field_t(void* f, const Geom& g, const float* field, const uint8_t* solid, size_t cell0,
-                                size_t cells, cudaStream_t s) {
+                                size_t cells, int layout, cudaStream_t s) {
     if (cells == 0) return cudaSuccess;
     const unsigned blocks = (unsigned)((cells + 255) / 256);
-    k_seed_field<Q, S><<<blocks, 256, 0, s>>>((typename S::T*)f, g.n, (const float4*)field, solid, cell0, cells);
+    k_seed_field<Q, S><<<blocks, 256, 0, s>>>((typename S::T*)f, g, (const float4*)field, solid, cell0, cells,
+                                              layout);
     return cudaGetLastError();
 }
 
@@ -214,13 +233,13 @@ static cudaError_t seed_field_t(void* f, const Geom& g, const float* field, cons
     } while (0)
 
 cudaError_t launch_seed_uniform(int q, int storage, void* f, const Geom& g, float rho, float ux, float uy, float uz,
-                                cudaStream_t s) {
-    FC_DISPATCH(q, storage, seed_uniform_t, f, g, rho, ux, uy, uz, s);
+                                int layout, cudaStream_t s) {
+    FC_DISPATCH(q, storage, seed_uniform_t, f, g, rho, ux, uy, uz, layout, s);
 }
 
 cudaError_t launch_seed_field(int q, int storage, void* f, const Geom& g, const float* field, const uint8_t* solid,
-                              size_t cell0, size_t cells, cudaStream_t s) {
-    FC_DISPATCH(q, storage, seed_field_t, f, g, field, solid, cell0, cells, s);
+                              size_t cell0, size_t cells, int layout, cudaStream_t s) {
+    FC_DISPATCH(q, storage, seed_field_t, f, g, field, solid, cell0, cells, layout, s);
 }
 
 cudaError_t launch_classify(int q, const uint8_t* solid, const Geom& g, uint8_t* flags, uint32_t* bulk_bits,

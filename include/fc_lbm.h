@@ -59,7 +59,10 @@ extern "C" {
 #define FC_STORAGE_BF16_OFFSET 2
 
 /* Streaming scheme. PINGPONG keeps two population copies (pull scheme, the
- * reference's layout); AA keeps one copy updated in place. */
+ * reference's layout); AA keeps one copy updated in place, half the device
+ * memory, with results bit-identical to PINGPONG. AA needs an even nx >= 4
+ * and does not combine with the learned closure, batches, closure samples
+ * or layer copies (FC_LBM_ERR_UNSUPPORTED). */
 #define FC_STREAMING_PINGPONG 0
 #define FC_STREAMING_AA 1
 
