@@ -60,7 +60,7 @@ CONFIGS = {
 }
 
 BYTES_PER_ELEM = {"fp32": 4, "fp16_offset": 2, "bf16_offset": 2, "fp16_learned": 2, "bf16_learned": 2,
-                  "fp32_aa": 4, "fp16_aa": 2, "bf16_aa": 2}
+                  "fp32_aa": 4, "fp16_aa": 2, "bf16_aa": 2, "fp16_tma": 2}
 # per-cell bytes beyond the populations: the closure's wall-distance byte
 EXTRA_BYTES = {"fp16_learned": 1, "bf16_learned": 1}
 CLOSURE_WEIGHTS = os.path.join(ROOT, "flowcraft_b200", "data", "closure_c4.json")
@@ -183,7 +183,7 @@ def storage_of(variant):
     from flowcraft_b200 import Storage
     return {"fp32": Storage.FP32, "fp16_offset": Storage.FP16_OFFSET, "bf16_offset": Storage.BF16_OFFSET,
             "fp16_learned": Storage.FP16_OFFSET, "bf16_learned": Storage.BF16_OFFSET, "fp32_aa": Storage.FP32,
-            "fp16_aa": Storage.FP16_OFFSET, "bf16_aa": Storage.BF16_OFFSET}[variant]
+            "fp16_aa": Storage.FP16_OFFSET, "bf16_aa": Storage.BF16_OFFSET, "fp16_tma": Storage.FP16_OFFSET}[variant]
 
 
 def streaming_of(variant):
@@ -196,7 +196,9 @@ def make_solver(cfg, solid, sdf, variant, device_index):
     from flowcraft_b200 import LatticeModel, LbmSolver, Params, VoxelGrid
     s = LbmSolver()
     grid = VoxelGrid(cfg["nx"], cfg["ny"], cfg["nz"], solid=solid, signedDistance=sdf)
-    if not s.Init(device_index, grid, LatticeModel.D3Q19, storage_of(variant), streaming_of(variant)):
+    from flowcraft_b200.lbm import OPTION_TMA_STAGING
+    flags = OPTION_TMA_STAGING if variant.endswith("_tma") else 0  # interior rows staged by TMA tensor copies
+    if not s.Init(device_index, grid, LatticeModel.D3Q19, storage_of(variant), streaming_of(variant), flags):
         raise RuntimeError(s.LastError())
     s.Reset(Params(tau=tau_for(cfg), inletVelocity=cfg["u"], smagorinskyCs=cfg["cs"]), True)
     if variant.endswith("_learned"):

@@ -31,6 +31,7 @@ struct fc_lbm {
     int model = FC_LATTICE_D3Q19;
     int storage = FC_STORAGE_FP32;
     int streaming = FC_STREAMING_PINGPONG;
+    int flags = 0;  // FC_OPTION_* bits
     Geom g{};
     fc_params params{0.8f, 0.05f, 0, 1, 1, 0.12f};  // LbmSolver::Params defaults (LbmSolver.h:61-100)
     cudaStream_t stream = nullptr;
@@ -356,7 +357,8 @@ cudaError_t launch_bulk(fc_lbm* h, const fc::StepParams& p, const void* fin, voi
     if (h->closure_on)
         return fc::launch_bulk_pull_learned(h->q, h->storage, fin, fout, h->d_bulk_bits, h->g, p, z0, zc,
                                             h->d_diverged, s, nl, h->closure);
-    return fc::launch_bulk_pull(h->q, h->storage, fin, fout, h->d_bulk_bits, h->g, p, z0, zc, h->d_diverged, s, nl);
+    return fc::launch_bulk_pull(h->q, h->storage, fin, fout, h->d_bulk_bits, h->g, p, z0, zc, h->d_diverged, s, nl,
+                                (h->flags & FC_OPTION_TMA_STAGING) ? 1 : 0);
 }
 
 cudaError_t launch_boundary(fc_lbm* h, const fc::StepParams& p, const void* fin, void* fout, uint32_t b, uint32_t e,
@@ -477,6 +479,7 @@ int fc_lbm_init(fc_lbm* h, const fc_grid_desc* grid, int32_t model, const fc_opt
     h->q = model == FC_LATTICE_D3Q19 ? 19 : 15;
     h->storage = o.storage;
     h->streaming = o.streaming;
+    h->flags = o.flags;
     h->g.nx = grid->nx;
     h->g.ny = grid->ny;
     h->g.nz = grid->nz;

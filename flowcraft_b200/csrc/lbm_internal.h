@@ -175,9 +175,19 @@ cudaError_t launch_boundary_aa(int q, int storage, void* f, const BoundaryList& 
 cudaError_t launch_aa_prime(int q, int storage, const void* f, const BoundaryList& bl, uint32_t count, const Geom& g,
                             const AaSide& sd, int par, cudaStream_t s);
 
+// `staged`: run the interior rows through k_bulk_tiles (8-row tiles staged
+// in shared memory by TMA tensor copies) when the lattice allows it
+// (staged_eligible), the rest through k_bulk_pairs.
 cudaError_t launch_bulk_pull(int q, int storage, const void* fin, void* fout, const uint32_t* bulk_bits,
                              const Geom& g, const StepParams& p, int z0, int zc, int* diverged, cudaStream_t s,
-                             int* launched);
+                             int* launched, int staged = 0);
+// The interior rows only (lbm_step_staged.cu): rows off the Y/Z faces,
+// 64-cell chunks off the row ends.
+cudaError_t launch_bulk_staged(int q, int storage, const void* fin, void* fout, const uint32_t* bulk_bits,
+                               const Geom& g, const StepParams& p, int z0, int zc, int* diverged, cudaStream_t s,
+                               int* launched);
+// nx a multiple of 16 bytes' worth of elements, nx > 128, ny, nz >= 3.
+bool staged_eligible(int storage, const Geom& g);
 cudaError_t launch_boundary_pull_learned(int q, int storage, const void* fin, void* fout, const BoundaryList& bl,
                                          uint32_t begin, uint32_t end, const Geom& g, const StepParams& p,
                                          int* diverged, cudaStream_t s, const ClosureDev& cl);

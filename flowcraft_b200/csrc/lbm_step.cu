@@ -218,29 +218,96 @@ __device__ __forceinline__ void plane_cell(const typename S::T* __restrict__ fin
 // row and every 64-cell chunk. A warp covers cells [64*blockIdx.x, +64) of one
 // row, so whether it touches a Y/Z domain face (`face`) or the first or last
 // chunk of the row (`edge`) is uniform across the warp:
-//   * interior warps run the pure pair pull (aligned 2-element loads for the
-//     e_x = 0 directions, pair stores);
-//   * face and edge warps run the general pair path: sources off the Y/Z edge
-//     come from the cell's own mirrored / bounced plane (the choice is per
-//     direction and uniform across the row), cells that are not bulk cells
-//     here keep in-bounds addresses and are not stored; the lane holding
-//     an x = 0 or x = nx-1 cell also updates that inlet / outlet cell.
+//   * interior warps, and the full pairs of edge warps off the faces, run
+//     the pure pair pull (aligned 2-element loads for the e_x = 0
+//     directions, pair stores);
+//   * face warps, and the partial pairs of edge warps, run the general pair
+//     path: sources off the Y/Z edge come from the cell's own mirrored /
+//     bounced plane (the choice is per direction and uniform across the
+//     row), cells that are not bulk cells here keep in-bounds addresses and
+//     are not stored;
+//   * the lane holding an x = 0 or x = nx-1 cell first updates that inlet /
+//     outlet cell.
+// Stores the pair's post-collision values (full floats for the exact
+// format, scaled offsets otherwise): one 2-element store per plane for a full
+// pair, element stores for the valid cell of a partial one.
+template <int Q, class S>
+__device__ __forceinline__ void store_pair(const PlanePtrs& pp, uint32_t c, const float2 (&v)[Q], unsigned pair) {
+    using L = Lattice<Q>;
+    using T = typename S::T;
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        T* dst = static_cast<T*>(pp.dst[i]);
+        typename S::T2 h;
+        if constexpr (S::kExact)
+            h = S::enc2(v[i].x, v[i].y, L::w(i));
+        else
+            h = S::pack2(v[i].x, v[i].y);
+        if (pair == 3u) {
+            *reinterpret_cast<typename S::T2*>(dst + c) = h;
+        } else {
+            if (pair & 1u) dst[c] = h.x;
+            if (pair & 2u) dst[c + 1u] = h.y;
+        }
+    });
+}
+
+// Blocks of k_bulk_pairs when its interior warps run in k_bulk_tiles: the
+// shell as a 1D list of (chunk, 8-row block, z) items in three regions,
+//   E  the first and last chunk of every row block of every layer,
+//   F  the other chunks of the row blocks that hold y = 0 or y = ny-1, in
+//      layers off the Z faces,
+//   G  the other chunks of every row block of the Z-face layers,
+// so no block is launched only to find nothing to do. n == 0: the whole
+// lattice, blockIdx = (chunk, row block, z - z0).
+struct PairsShell {
+    unsigned long long n, ne, nf;  // items in all, in E, in F
+    int gx, nyb;                   // chunks per row, 8-row blocks per layer
+    int z0, zi0;                   // first layer of the range, first layer off the Z faces
+    int nyf;                       // row blocks in F (1 or 2)
+    int nzf, zf[2];                // Z-face layers in the range
+};
+
+__device__ __forceinline__ void shell_item(const PairsShell& sh, int& bx, int& by, int& z) {
+    unsigned long long it = blockIdx.x;
+    if (it < sh.ne) {
+        bx = (it & 1ull) ? sh.gx - 1 : 0;
+        const unsigned long long r = it >> 1;
+        by = (int)(r % sh.nyb);
+        z = sh.z0 + (int)(r / sh.nyb);
+        return;
+    }
+    it -= sh.ne;
+    const int inner = sh.gx - 2;
+    bx = 1 + (int)(it % inner);
+    const unsigned long long r = it / inner;
+    if (it < sh.nf) {
+        by = (r % sh.nyf) ? sh.nyb - 1 : 0;
+        z = sh.zi0 + (int)(r / sh.nyf);
+    } else {
+        const unsigned long long q = r - sh.nf / inner;
+        by = (int)(q % sh.nyb);
+        z = (q / sh.nyb) ? sh.zf[1] : sh.zf[0];
+    }
+}
+
 template <int Q, class S>
 __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs(const typename S::T* __restrict__ fin,
                                                                 typename S::T* __restrict__ fout,
                                                                 const uint32_t* __restrict__ bulk_bits, Geom g,
                                                                 StepParams p, PlanePtrs pp, int z0,
-                                                                int* __restrict__ diverged) {
+                                                                int* __restrict__ diverged, PairsShell sh) {
     using L = Lattice<Q>;
     using T = typename S::T;
-    const int y = blockIdx.y * kBulkRows + threadIdx.y;
-    const int z = z0 + blockIdx.z;
+    int bx = blockIdx.x, by = blockIdx.y, z = z0 + blockIdx.z;
+    if (sh.n) shell_item(sh, bx, by, z);
+    const int y = by * kBulkRows + threadIdx.y;
     if (y >= g.ny) return;
     const size_t row = (size_t)z * g.ny + y;
     const int k = 2 * threadIdx.x;
-    const int w = 2 * blockIdx.x + (k >> 5);
+    const int w = 2 * bx + (k >> 5);
     const uint32_t bits = w < g.wpr ? __ldg(bulk_bits + row * g.wpr + w) : 0u;
-    const int x = 64 * blockIdx.x + k;
+    const int x = 64 * bx + k;
     unsigned pair = (bits >> (k & 31)) & 3u;
     unsigned plane = 0;  // fluid inlet / outlet cells of this pair
     if (x == 0) {
@@ -254,15 +321,24 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs(const typename
     if (!(pair | plane)) return;
     const uint32_t c = (uint32_t)(row * g.nx + x);
     const bool face = (y == 0) | (y == g.ny - 1) | (z == 0) | (z == g.nz - 1);
-    const bool edge = (blockIdx.x == 0) | (64 * (int)blockIdx.x + 64 >= g.nx);
+    const bool edge = (bx == 0) | (64 * bx + 64 >= g.nx);
+    if (sh.n && !face && !edge) return;  // an interior warp: done by k_bulk_tiles
 
+    // the one lane of a row end that holds an inlet or outlet cell finishes it alone
+    if (plane) plane_cell<Q, S>(fin, fout, g, p, plane == 1u ? x : x + 1, plane == 1u ? c : (size_t)c + 1);
+    if (!pair) return;
     float2 v[Q];
-    if (!face && !edge) {
-        if (pair != 3u) {  // one of the two is next to a wall (a boundary-list cell)
+    if (!face) {
+        if (pair != 3u && !edge) {  // one of the two is next to a wall (a boundary-list cell)
             const uint32_t cc = pair == 1u ? c : c + 1u;
             bulk_cell<Q, S, false>(fin, fout, g, p, x + (pair == 1u ? 0 : 1), y, z, cc, diverged);
             return;
         }
+        // Full pairs, and in row-end warps every pair: the plain pull. Off the
+        // Y/Z faces every source of a row lies inside the population set, also
+        // for a cell that is not stored here (an inlet / outlet or wall cell
+        // next to a pair cell), so a row-end warp runs one uniform path, with
+        // the masked pair collision of the general path for its partial pairs.
         static_for<0, Q>([&](auto I) {
             constexpr int i = decltype(I)::value;
             const T* src = static_cast<const T*>(pp.src[i]);
@@ -275,21 +351,11 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs(const typename
                                      : make_float2(S::raw(S::ld(src + c)), S::raw(S::ld(src + c + 1u)));
             }
         });
-        if (collide_pair<Q, S>(v, p.tau, p.cs)) atomicOr(diverged, 1);
-        static_for<0, Q>([&](auto I) {
-            constexpr int i = decltype(I)::value;
-            T* dst = static_cast<T*>(pp.dst[i]);
-            if constexpr (S::kExact)
-                *reinterpret_cast<typename S::T2*>(dst + c) = S::enc2(v[i].x, v[i].y, L::w(i));
-            else
-                *reinterpret_cast<typename S::T2*>(dst + c) = S::pack2(v[i].x, v[i].y);
-        });
+        if (collide_pair<Q, S>(v, p.tau, p.cs) & pair) atomicOr(diverged, 1);
+        store_pair<Q, S>(pp, c, v, pair);
         return;
     }
-    // general pair path (face rows, first / last chunk of a row); the one
-    // lane of a row end that holds an inlet or outlet cell finishes it alone
-    if (plane) plane_cell<Q, S>(fin, fout, g, p, plane == 1u ? x : x + 1, plane == 1u ? c : (size_t)c + 1);
-    if (!pair) return;
+    // general pair path: face rows, and partial pairs of the row-end chunks
     const bool va = pair & 1u, vb = pair & 2u;
     static_for<0, Q>([&](auto I) {
         constexpr int i = decltype(I)::value;
@@ -309,25 +375,7 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs(const typename
     });
     const unsigned bad = collide_pair<Q, S>(v, p.tau, p.cs) & pair;
     if (bad) atomicOr(diverged, 1);
-    static_for<0, Q>([&](auto I) {
-        constexpr int i = decltype(I)::value;
-        T* dst = static_cast<T*>(pp.dst[i]);
-        if (pair == 3u) {
-            if constexpr (S::kExact)
-                *reinterpret_cast<typename S::T2*>(dst + c) = S::enc2(v[i].x, v[i].y, L::w(i));
-            else
-                *reinterpret_cast<typename S::T2*>(dst + c) = S::pack2(v[i].x, v[i].y);
-        } else {
-            if constexpr (S::kExact) {
-                if (va) dst[c] = S::enc(v[i].x, L::w(i));
-                if (vb) dst[c + 1u] = S::enc(v[i].y, L::w(i));
-            } else {
-                const typename S::T2 h = S::pack2(v[i].x, v[i].y);
-                if (va) dst[c] = h.x;
-                if (vb) dst[c + 1u] = h.y;
-            }
-        }
-    });
+    store_pair<Q, S>(pp, c, v, pair);
 }
 
 // k_bulk_pairs with the learned closure (16-bit offset storage). The MLP is a
@@ -370,15 +418,15 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned(const 
     // both cells' wall distances in one aligned load (x and nx are even)
     const unsigned wd = pair ? (unsigned)__ldg(reinterpret_cast<const unsigned short*>(cl.wall + c)) : 0xffffu;
     const bool face = (y == 0) | (y == g.ny - 1) | (z == 0) | (z == g.nz - 1);
-    const bool edge = (blockIdx.x == 0) | (64 * (int)blockIdx.x + 64 >= g.nx);
     if (plane) plane_cell<Q, S>(fin, fout, g, p, plane == 1u ? x : x + 1, plane == 1u ? c : (size_t)c + 1);
     const bool va = pair & 1u, vb = pair & 2u;
 
-    // The load path is chosen per warp: the pure pair pull when every lane
-    // holds a full bulk pair or nothing, the masked general path otherwise.
-    // Lanes without a pair load from in-bounds addresses too (their own row)
-    // and store nothing, so neither path diverges.
-    const bool fast = !face && !edge && __all_sync(0xffffffffu, pair == 3u || pair == 0u);
+    // The load path is chosen per warp: off the Y/Z faces every lane takes
+    // the pure pair pull (every source of a row off the faces lies inside the
+    // lattice, also for the cells a lane does not store: the inlet / outlet
+    // cell of a row end and wall cells), the masked general path on the faces.
+    // Lanes beyond the row load their own row and store nothing.
+    const bool fast = !face;
     const uint32_t cs = x < g.nx ? c : (uint32_t)(row * g.nx);
     float2 v[Q];
     if (fast) {
@@ -570,9 +618,11 @@ __global__ void __launch_bounds__(32 * ROWS, 32 / ROWS) k_bulk_pairs_batch(const
         const uint32_t c = (uint32_t)(row * g.nx + x);
         const bool face = (y == 0) | (y == g.ny - 1) | (z == 0) | (z == g.nz - 1);
         const bool edge = (bx == 0) | (64 * bx + 64 >= g.nx);
+        if (plane) plane_cell<Q, S>(fin, fout, g, p, plane == 1u ? x : x + 1, plane == 1u ? c : (size_t)c + 1);
+        if (!pair) continue;
         float2 v[Q];
-        if (!face && !edge) {
-            if (pair != 3u) {
+        if (!face) {  // as k_bulk_pairs
+            if (pair != 3u && !edge) {
                 const uint32_t cc = pair == 1u ? c : c + 1u;
                 bulk_cell<Q, S, false>(fin, fout, g, p, x + (pair == 1u ? 0 : 1), y, z, cc, sl.diverged);
                 continue;
@@ -589,19 +639,10 @@ __global__ void __launch_bounds__(32 * ROWS, 32 / ROWS) k_bulk_pairs_batch(const
                                          : make_float2(S::raw(S::ld(src + c)), S::raw(S::ld(src + c + 1u)));
                 }
             });
-            if (collide_pair<Q, S>(v, p.tau, p.cs)) atomicOr(sl.diverged, 1);
-            static_for<0, Q>([&](auto I) {
-                constexpr int i = decltype(I)::value;
-                T* dst = static_cast<T*>(pp.dst[i]);
-                if constexpr (S::kExact)
-                    *reinterpret_cast<typename S::T2*>(dst + c) = S::enc2(v[i].x, v[i].y, L::w(i));
-                else
-                    *reinterpret_cast<typename S::T2*>(dst + c) = S::pack2(v[i].x, v[i].y);
-            });
+            if (collide_pair<Q, S>(v, p.tau, p.cs) & pair) atomicOr(sl.diverged, 1);
+            store_pair<Q, S>(pp, c, v, pair);
             continue;
         }
-        if (plane) plane_cell<Q, S>(fin, fout, g, p, plane == 1u ? x : x + 1, plane == 1u ? c : (size_t)c + 1);
-        if (!pair) continue;
         const bool va = pair & 1u, vb = pair & 2u;
         static_for<0, Q>([&](auto I) {
             constexpr int i = decltype(I)::value;
@@ -621,25 +662,7 @@ __global__ void __launch_bounds__(32 * ROWS, 32 / ROWS) k_bulk_pairs_batch(const
         });
         const unsigned bad = collide_pair<Q, S>(v, p.tau, p.cs) & pair;
         if (bad) atomicOr(sl.diverged, 1);
-        static_for<0, Q>([&](auto I) {
-            constexpr int i = decltype(I)::value;
-            T* dst = static_cast<T*>(pp.dst[i]);
-            if (pair == 3u) {
-                if constexpr (S::kExact)
-                    *reinterpret_cast<typename S::T2*>(dst + c) = S::enc2(v[i].x, v[i].y, L::w(i));
-                else
-                    *reinterpret_cast<typename S::T2*>(dst + c) = S::pack2(v[i].x, v[i].y);
-            } else {
-                if constexpr (S::kExact) {
-                    if (va) dst[c] = S::enc(v[i].x, L::w(i));
-                    if (vb) dst[c + 1u] = S::enc(v[i].y, L::w(i));
-                } else {
-                    const typename S::T2 h = S::pack2(v[i].x, v[i].y);
-                    if (va) dst[c] = h.x;
-                    if (vb) dst[c + 1u] = h.y;
-                }
-            }
-        });
+        store_pair<Q, S>(pp, c, v, pair);
     }
 }
 
@@ -858,24 +881,55 @@ __global__ void __launch_bounds__(128) k_boundary_pull_learned(const typename S:
     });
 }
 
+// Plane pointers of a ping-pong step (PlanePtrs in lbm_internal.h).
+template <int Q, class S>
+static PlanePtrs pp_of(const void* fin, void* fout, const Geom& g) {
+    PlanePtrs pp{};
+    for (int i = 0; i < Q; ++i) {
+        const long long off = (long long)Lattice<Q>::ex(i) + (long long)Lattice<Q>::ey(i) * g.nx +
+                              (long long)Lattice<Q>::ez(i) * g.nxy;
+        pp.src[i] = (const typename S::T*)fin + ((long long)i * (long long)g.n - off);
+        pp.dst[i] = (typename S::T*)fout + (size_t)i * g.n;
+    }
+    return pp;
+}
+
 template <int Q, class S>
 static cudaError_t bulk_t(const void* fin, void* fout, const uint32_t* bits, const Geom& g, const StepParams& p,
-                          int z0, int zc, int* dv, cudaStream_t s, int* launched) {
+                          int z0, int zc, int* dv, cudaStream_t s, int* launched, int staged) {
     *launched = 0;
     if (zc <= 0) return cudaSuccess;
     const int z1 = z0 + zc;
     dim3 block(32, kBulkRows, 1);
     if (g.nx % 2 == 0) {  // pairs start on even cells: every row through k_bulk_pairs
-        PlanePtrs pp{};
-        for (int i = 0; i < Q; ++i) {
-            const long long off = (long long)Lattice<Q>::ex(i) + (long long)Lattice<Q>::ey(i) * g.nx +
-                                  (long long)Lattice<Q>::ez(i) * g.nxy;
-            pp.src[i] = (const typename S::T*)fin + ((long long)i * (long long)g.n - off);
-            pp.dst[i] = (typename S::T*)fout + (size_t)i * g.n;
+        PairsShell sh{};
+        if (staged) {  // the interior warps' rows staged in shared memory by TMA
+            int nl = 0;
+            cudaError_t e = launch_bulk_staged(Q, storage_code<S>(), fin, fout, bits, g, p, z0, zc, dv, s, &nl);
+            if (e != cudaSuccess) return e;
+            *launched += nl;
+            sh.gx = (g.nx + 63) / 64;
+            sh.nyb = (g.ny + kBulkRows - 1) / kBulkRows;
+            sh.z0 = z0;
+            sh.zi0 = z0 > 1 ? z0 : 1;
+            const int zi1 = z1 < g.nz - 1 ? z1 : g.nz - 1;
+            sh.nyf = sh.nyb >= 2 ? 2 : 1;
+            sh.nzf = 0;
+            if (z0 <= 0 && 0 < z1) sh.zf[sh.nzf++] = 0;
+            if (g.nz > 1 && z0 <= g.nz - 1 && g.nz - 1 < z1) sh.zf[sh.nzf++] = g.nz - 1;
+            sh.ne = 2ull * sh.nyb * zc;
+            sh.nf = zi1 > sh.zi0 ? (unsigned long long)(sh.gx - 2) * sh.nyf * (zi1 - sh.zi0) : 0ull;
+            const unsigned long long ng = (unsigned long long)(sh.gx - 2) * sh.nyb * sh.nzf;
+            sh.n = sh.ne + sh.nf + ng;
+            if (sh.n == 0) return cudaSuccess;
+            k_bulk_pairs<Q, S><<<(unsigned)sh.n, block, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout, bits, g,
+                                                                p, pp_of<Q, S>(fin, fout, g), z0, dv, sh);
+            ++*launched;
+            return cudaGetLastError();
         }
         dim3 grid((unsigned)((g.nx + 63) / 64), (unsigned)((g.ny + kBulkRows - 1) / kBulkRows), (unsigned)zc);
-        k_bulk_pairs<Q, S><<<grid, block, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout, bits, g, p, pp, z0,
-                                                  dv);
+        k_bulk_pairs<Q, S><<<grid, block, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout, bits, g, p,
+                                                  pp_of<Q, S>(fin, fout, g), z0, dv, sh);
         ++*launched;
         return cudaGetLastError();
     }
@@ -996,8 +1050,9 @@ static cudaError_t closure_probe_t(const void* f, const Geom& g, const ClosureDe
 
 cudaError_t launch_bulk_pull(int q, int storage, const void* fin, void* fout, const uint32_t* bulk_bits,
                              const Geom& g, const StepParams& p, int z0, int zc, int* diverged, cudaStream_t s,
-                             int* launched) {
-    FC_DISPATCH(q, storage, bulk_t, fin, fout, bulk_bits, g, p, z0, zc, diverged, s, launched);
+                             int* launched, int staged) {
+    const int st = staged && g.nx % 2 == 0 && staged_eligible(storage, g) ? 1 : 0;
+    FC_DISPATCH(q, storage, bulk_t, fin, fout, bulk_bits, g, p, z0, zc, diverged, s, launched, st);
 }
 
 cudaError_t launch_boundary_pull(int q, int storage, const void* fin, void* fout, const BoundaryList& bl,

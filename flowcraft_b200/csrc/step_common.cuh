@@ -7,6 +7,8 @@
 #include "lbm_internal.h"
 #include "storage.cuh"
 
+#include <type_traits>
+
 namespace fc {
 
 constexpr int kBulkRows = 8;  // block = 32 x-lanes x 8 rows
@@ -55,6 +57,12 @@ __device__ __forceinline__ unsigned collide_pair(float2 (&v)[Q], float tau, floa
     } else {
         return collide_offsets2<Q>(v, tau, cs);
     }
+}
+
+// Storage code of a format (0 FP32, 1 FP16 offset, 2 BF16 offset).
+template <class S>
+constexpr int storage_code() {
+    return S::kBytes == 4 ? 0 : (std::is_same<S, StoreF16>::value ? 1 : 2);
 }
 
 }  // namespace fc

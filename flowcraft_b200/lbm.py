@@ -70,9 +70,14 @@ class _Params(ctypes.Structure):
     ]
 
 
+# fc_options.flags: stage the interior rows in shared memory by TMA tensor
+# copies (16-bit formats; identical results, off by default)
+OPTION_TMA_STAGING = 1
+
+
 class _Options(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("storage", ctypes.c_int32),
-                ("streaming", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("streaming", ctypes.c_int32), ("flags", ctypes.c_int32)]
 
 
 class _Stats(ctypes.Structure):
@@ -312,7 +317,7 @@ class LbmSolver:
         return self._h
 
     def Init(self, device, grid: VoxelGrid, model: LatticeModel = LatticeModel.D3Q19,
-             storage: Storage = Storage.FP32, streaming: Streaming = Streaming.PINGPONG) -> bool:
+             storage: Storage = Storage.FP32, streaming: Streaming = Streaming.PINGPONG, flags: int = 0) -> bool:
         """LbmSolver::Init (LbmSolver.cpp:205-366); ``device`` is a CUDA ordinal."""
         self._device = int(device)
         desc = _GridDesc()
@@ -342,7 +347,7 @@ class LbmSolver:
                 desc.signed_distance = sdf.ctypes.data
                 keep.append(sdf)
             self._solid_cpu = solid.copy()
-        opts = _Options(int(device), int(storage), int(streaming), 0)
+        opts = _Options(int(device), int(storage), int(streaming), int(flags))
         rc = self._lib.fc_lbm_init(self._h, ctypes.byref(desc), int(model), ctypes.byref(opts))
         if rc == FC_LBM_OK:
             self._model = LatticeModel(model)

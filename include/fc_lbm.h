@@ -97,11 +97,19 @@ typedef struct fc_params {
     float smagorinsky_cs;
 } fc_params;
 
+/* fc_options.flags bits. TMA_STAGING runs the interior rows of the
+ * ping-pong bulk step (16-bit formats, nx a multiple of 8 above 128, ny, nz
+ * >= 3) through a kernel that stages 8-row tiles of the source rows in
+ * shared memory with TMA tensor copies, instead of loading them directly;
+ * results are identical. It is off by default: on B200 the direct loads are
+ * faster (the step is issue-bound, not latency-bound). */
+#define FC_OPTION_TMA_STAGING 1
+
 typedef struct fc_options {
     int32_t device;    /* CUDA device ordinal */
     int32_t storage;   /* FC_STORAGE_* */
     int32_t streaming; /* FC_STREAMING_* */
-    int32_t reserved;
+    int32_t flags;     /* FC_OPTION_* bits, 0 for the defaults */
 } fc_options;
 
 /* LbmSolver::Stats (FlowCraft/LbmSolver.h:172-184) plus the FP64 sums the
