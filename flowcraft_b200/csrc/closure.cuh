@@ -83,20 +83,39 @@ __device__ __forceinline__ void mma_k16(float (&d)[4], uint32_t a0, uint32_t a1,
 }
 
 // Raw inputs 0-2 of one cell from its Pi_neq, |Pi|^2 (pp) and 1/rho.
-__device__ __forceinline__ void closure_invariants(float pxx, float pyy, float pzz, float pxy, float pxz, float pyz,
-                                                   float pp, float inv_rho, float& x0, float& x1, float& x2) {
-    const float r = pp > 0.0f ? rsqrtf(pp) : 0.0f;  // 1/|Pi|
-    const float mag = pp * r;                       // |Pi|
-    x0 = __log2f(fmaf(mag, inv_rho, 1e-12f));
+// Input 0 alone; r receives 1/|Pi| for closure_x12.
+__device__ __forceinline__ float closure_x0(float pp, float inv_rho, float& r) {
+    r = pp > 0.0f ? rsqrtf(pp) : 0.0f;  // 1/|Pi|
+    const float mag = pp * r;           // |Pi|
+    return __log2f(fmaf(mag, inv_rho, 1e-12f));
+}
+
+// Inputs 1 and 2 from Pi_neq and r = 1/|Pi|.
+__device__ __forceinline__ void closure_x12(float pxx, float pyy, float pzz, float pxy, float pxz, float pyz, float r,
+                                            float& x1, float& x2) {
     x1 = (pxx + pyy + pzz) * r;
     const float det = pxx * fmaf(pyy, pzz, -pyz * pyz) - pxy * fmaf(pxy, pzz, -pyz * pxz) +
                       pxz * fmaf(pxy, pyz, -pyy * pxz);
     x2 = det * (r * r * r);
 }
 
+__device__ __forceinline__ void closure_invariants(float pxx, float pyy, float pzz, float pxy, float pxz, float pyz,
+                                                   float pp, float inv_rho, float& x0, float& x1, float& x2) {
+    float r;
+    x0 = closure_x0(pp, inv_rho, r);
+    closure_x12(pxx, pyy, pzz, pxy, pxz, pyz, r, x1, x2);
+}
+
+__device__ __forceinline__ bool closure_x0_in_range(const ClosureDev& cl, float x0) {
+    return x0 >= cl.lo[0] && x0 <= cl.hi[0];
+}
+
+__device__ __forceinline__ bool closure_x12_in_range(const ClosureDev& cl, float x1, float x2) {
+    return x1 >= cl.lo[1] && x1 <= cl.hi[1] && x2 >= cl.lo[2] && x2 <= cl.hi[2];
+}
+
 __device__ __forceinline__ bool closure_in_range(const ClosureDev& cl, float x0, float x1, float x2) {
-    return x0 >= cl.lo[0] && x0 <= cl.hi[0] && x1 >= cl.lo[1] && x1 <= cl.hi[1] && x2 >= cl.lo[2] &&
-           x2 <= cl.hi[2];
+    return closure_x0_in_range(cl, x0) && closure_x12_in_range(cl, x1, x2);
 }
 
 // Packs a cell's five normalized inputs and the constant 1 that carries the
@@ -120,8 +139,11 @@ __device__ __forceinline__ void closure_pack_inputs(const ClosureDev& cl, float 
 // __syncwarp, before the call) and receives (nu_A, nu_B). Every lane of the
 // warp must call it together. Row r of row tile j is cell A (r < 8) or B
 // (r >= 8) of lane 8j + (r & 7).
+// `tiles`: bit j set when row tile j (the cells of lanes 8j .. 8j+7) has a
+// cell that needs nu_t; cleared tiles are skipped (warp-uniform) and their
+// lanes receive whatever s_out held.
 __device__ __forceinline__ float2 closure_warp_mlp(const uint4* __restrict__ wt, const uint32_t* s_in,
-                                                   float2* s_out) {
+                                                   float2* s_out, unsigned tiles = 0xfu) {
     const int lane = threadIdx.x & 31;
     const int gq = lane >> 2, tq = lane & 3;
     // the small operands stay in registers across the four row tiles; each
@@ -136,6 +158,7 @@ __device__ __forceinline__ float2 closure_warp_mlp(const uint4* __restrict__ wt,
     const uint32_t one = tq == 0 ? 0x3f80u : 0u;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
+        if (!((tiles >> j) & 1u)) continue;
         const int src = 8 * j + gq;
         const uint32_t a0 = s_in[src * 8 + tq];      // cell A of lane src: row gq
         const uint32_t a1 = s_in[src * 8 + 4 + tq];  // cell B: row gq + 8

@@ -415,8 +415,6 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned(const 
         pair &= ~2u;
     }
     const uint32_t c = (uint32_t)(row * g.nx + x);
-    // both cells' wall distances in one aligned load (x and nx are even)
-    const unsigned wd = pair ? (unsigned)__ldg(reinterpret_cast<const unsigned short*>(cl.wall + c)) : 0xffffu;
     const bool face = (y == 0) | (y == g.ny - 1) | (z == 0) | (z == g.nz - 1);
     if (plane) plane_cell<Q, S>(fin, fout, g, p, plane == 1u ? x : x + 1, plane == 1u ? c : (size_t)c + 1);
     const bool va = pair & 1u, vb = pair & 2u;
@@ -454,26 +452,43 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned(const 
     Mom2 mo;
     const unsigned bad = moments2<Q>(v, mo) & pair;
     // everything besides nu_t is settled before the MMA, so only the moments
-    // stay live across it
-    float xa0, xa1, xa2, xb0, xb1, xb2;
-    closure_invariants(mo.pxx.x, mo.pyy.x, mo.pzz.x, mo.pxy.x, mo.pxz.x, mo.pyz.x, mo.pp.x, mo.inv.x, xa0, xa1, xa2);
-    closure_invariants(mo.pxx.y, mo.pyy.y, mo.pzz.y, mo.pxy.y, mo.pxz.y, mo.pyz.y, mo.pp.y, mo.inv.y, xb0, xb1, xb2);
-    const bool la = closure_in_range(cl, xa0, xa1, xa2), lb = closure_in_range(cl, xb0, xb1, xb2);
+    // stay live across it. The range test goes input by input, each stage
+    // only in warps where some lane is still in range (warp votes, so the
+    // branches stay uniform); the inputs are packed for the MLP only where
+    // it runs.
+    float ra, rb;
+    const float xa0 = closure_x0(mo.pp.x, mo.inv.x, ra), xb0 = closure_x0(mo.pp.y, mo.inv.y, rb);
+    bool la = closure_x0_in_range(cl, xa0), lb = closure_x0_in_range(cl, xb0);
+    float xa1 = 0.0f, xa2 = 0.0f, xb1 = 0.0f, xb2 = 0.0f;
+    if (__any_sync(0xffffffffu, la || lb)) {
+        closure_x12(mo.pxx.x, mo.pyy.x, mo.pzz.x, mo.pxy.x, mo.pxz.x, mo.pyz.x, ra, xa1, xa2);
+        closure_x12(mo.pxx.y, mo.pyy.y, mo.pzz.y, mo.pxy.y, mo.pxz.y, mo.pyz.y, rb, xb1, xb2);
+        la = la && closure_x12_in_range(cl, xa1, xa2);
+        lb = lb && closure_x12_in_range(cl, xb1, xb2);
+    }
     // the Smagorinsky fallback only where some lane of the warp needs it
     float sga = 0.0f, sgb = 0.0f;
     if (__any_sync(0xffffffffu, !(la && lb))) {
         sga = smagorinsky_g(mo.pp.x, mo.rho.x, mo.inv.x, p.tau, p.cs);
         sgb = smagorinsky_g(mo.pp.y, mo.rho.y, mo.inv.y, p.tau, p.cs);
     }
-    uint32_t* in = &s_in[threadIdx.y][threadIdx.x * 8];
-    closure_pack_inputs(cl, xa0, xa1, xa2, (float)(wd & 0xffu) * 0.0625f, in);
-    closure_pack_inputs(cl, xb0, xb1, xb2, (float)(wd >> 8) * 0.0625f, in + 4);
-    __syncwarp();
     // A cell outside the training range takes the Smagorinsky value, so a
     // warp with no cell in range has no use for the MLP and skips it (the
-    // result is the same); the vote keeps the branch warp-uniform.
+    // result is the same).
     float2 nu = make_float2(0.0f, 0.0f);
-    if (__any_sync(0xffffffffu, la || lb)) nu = closure_warp_mlp(cl.frag, s_in[threadIdx.y], s_out[threadIdx.y]);
+    const unsigned need = __ballot_sync(0xffffffffu, la || lb);
+    if (need) {
+        // row tiles of the MLP (8 lanes each) with a cell in range
+        const unsigned tiles = ((need & 0xffu) ? 1u : 0u) | ((need & 0xff00u) ? 2u : 0u) |
+                               ((need & 0xff0000u) ? 4u : 0u) | ((need & 0xff000000u) ? 8u : 0u);
+        // both cells' wall distances in one aligned load (x and nx are even)
+        const unsigned wd = pair ? (unsigned)__ldg(reinterpret_cast<const unsigned short*>(cl.wall + c)) : 0xffffu;
+        uint32_t* in = &s_in[threadIdx.y][threadIdx.x * 8];
+        closure_pack_inputs(cl, xa0, xa1, xa2, (float)(wd & 0xffu) * 0.0625f, in);
+        closure_pack_inputs(cl, xb0, xb1, xb2, (float)(wd >> 8) * 0.0625f, in + 4);
+        __syncwarp();
+        nu = closure_warp_mlp(cl.frag, s_in[threadIdx.y], s_out[threadIdx.y], tiles);
+    }
     if (!pair) return;
     float2 gr;
     gr.x = la ? (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.x, p.tau))) * 4.5f : sga;
