@@ -67,6 +67,18 @@ struct fc_lbm {
     std::vector<uint8_t> solid_cpu;
     uint64_t steps_since_reset = 0;
     uint64_t launches = 0;
+    // asynchronous field readback: a snapshot kernel on rb_stream into
+    // d_snap, then the host copy; ev_snap marks the snapshot kernel's end
+    float* d_snap = nullptr;
+    cudaStream_t rb_stream = nullptr;
+    cudaEvent_t ev_snap = nullptr, ev_rb = nullptr;
+    bool rb_pending = false;
+    int snap_set = -1;  // population set the pending snapshot reads
+    // smoke-trail particles (particles.cu)
+    fc::ParticleSet parts{nullptr, nullptr, nullptr, 0, 0};
+    float* d_part_io = nullptr;  // count * length * 3 floats: trail readout / position upload
+    int* d_part_lens = nullptr;
+    unsigned long long part_seed = 0, part_counter = 0;
 };
 
 namespace {
@@ -176,6 +188,17 @@ fc::StepParams step_params(const fc_lbm* h) {
 
 void release(fc_lbm* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->rb_stream) {
+        cudaStreamSynchronize(h->rb_stream);
+        cudaStreamDestroy(h->rb_stream);
+        h->rb_stream = nullptr;
+    }
+    if (h->ev_snap) cudaEventDestroy(h->ev_snap);
+    if (h->ev_rb) cudaEventDestroy(h->ev_rb);
+    h->ev_snap = h->ev_rb = nullptr;
+    h->rb_pending = false;
+    h->snap_set = -1;
+    dfree(h->d_snap);
     if (h->pop[1] == h->pop[0]) h->pop[1] = nullptr;  // one in-place set
     dfree(h->pop[0]);
     dfree(h->pop[1]);
@@ -195,6 +218,12 @@ void release(fc_lbm* h) {
     dfree(h->d_wall);
     dfree(h->d_aa_bz);
     dfree(h->d_aa_outm);
+    dfree(h->parts.trail);
+    dfree(h->parts.head);
+    dfree(h->parts.len);
+    dfree(h->d_part_io);
+    dfree(h->d_part_lens);
+    h->parts.count = h->parts.length = 0;
     h->closure_on = false;
     dfree(h->d_stage);
     if (h->h_stage) cudaFreeHost(h->h_stage);
@@ -348,6 +377,14 @@ int aa_prime(fc_lbm* h) {
     return FC_LBM_OK;
 }
 
+// Work on stream s that overwrites population set `set` waits until a
+// pending asynchronous readback's snapshot kernel has read it.
+int guard_snapshot(fc_lbm* h, cudaStream_t s, int set) {
+    if (h->rb_pending && (in_place(h) || set == h->snap_set))
+        FC_TRY(h, cudaStreamWaitEvent(s, h->ev_snap, 0), "order after readback snapshot");
+    return FC_LBM_OK;
+}
+
 // The two step kernels, with or without the learned closure, ping-pong or in place.
 cudaError_t launch_bulk(fc_lbm* h, const fc::StepParams& p, const void* fin, void* fout, int z0, int zc,
                         cudaStream_t s, int* nl) {
@@ -380,6 +417,7 @@ int step_range_on(fc_lbm* h, cudaStream_t s, int z0, int zc) {
     const fc::StepParams p = step_params(h);
     const void* fin = h->pop[h->cur];
     void* fout = h->pop[1 - h->cur];
+    FC_RC(guard_snapshot(h, s, 1 - h->cur));
     if (h->n_bulk > 0) {
         int nl = 0;
         FC_TRY(h, launch_bulk(h, p, fin, fout, z0, z1 - z0, s, &nl), "bulk step");
@@ -581,6 +619,7 @@ int fc_lbm_reset(fc_lbm* h, const fc_params* params, int32_t seed_mid) {
         rho = 1.0f + 3.0f * dev;
     }
     h->cur = 0;
+    FC_RC(guard_snapshot(h, h->stream, 0));
     FC_TRY(h, fc::launch_seed_uniform(h->q, h->storage, h->pop[0], h->g, rho, ux, 0.0f, 0.0f, layout_of(h), h->stream),
            "seed");
     FC_TRY(h, cudaMemsetAsync(h->d_diverged, 0, sizeof(int), h->stream), "clear flag");
@@ -596,6 +635,7 @@ int fc_lbm_reset_from_field(fc_lbm* h, const float* field, size_t count) {
         return fail(h, FC_LBM_ERR_INVALID_ARG, "field must hold exactly 4 floats per cell");
     DeviceGuard dg(h->device);
     h->cur = 0;
+    FC_RC(guard_snapshot(h, h->stream, 0));
     const size_t chunk = h->stage_floats / 4;
     for (size_t c0 = 0; c0 < h->g.n; c0 += chunk) {
         const size_t nc = std::min(chunk, h->g.n - c0);
@@ -894,6 +934,7 @@ int fc_lbm_layer_copy(fc_lbm* h, int32_t z, int32_t next, void* buffer, int32_t 
     char* pop = static_cast<char*>(h->pop[next ? 1 - h->cur : h->cur]) + (size_t)z * width;
     cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
     FC_RC(enter_stream(h, s));
+    if (!to_buffer) FC_RC(guard_snapshot(h, s, next ? 1 - h->cur : h->cur));
     // one strided copy: Q planes of one layer <-> Q contiguous rows
     const cudaError_t e = to_buffer ? cudaMemcpy2DAsync(buffer, width, pop, pitch, width, (size_t)h->q,
                                                         cudaMemcpyDeviceToDevice, s)
@@ -1016,6 +1057,8 @@ int fc_lbm_step_timed(fc_lbm* h, int32_t n, float* total_ms, float* bulk_ms, flo
         const fc::StepParams p = step_params(h);
         const void* fin = h->pop[h->cur];
         void* fout = h->pop[1 - h->cur];
+        rc = guard_snapshot(h, h->stream, 1 - h->cur);
+        if (rc != FC_LBM_OK) break;
         cudaEventRecord(ev[2 + 4 * k], h->stream);
         cudaError_t ce = cudaSuccess;
         if (h->n_bulk > 0) {
@@ -1094,6 +1137,7 @@ int fc_lbm_load_populations(fc_lbm* h, const float* in, size_t count) {
             std::memcpy(h->h_stage + (size_t)i * nc, in + (size_t)i * h->g.n + c0, nc * sizeof(float));
         FC_TRY(h, cudaMemcpyAsync(h->d_stage, h->h_stage, nc * h->q * sizeof(float), cudaMemcpyHostToDevice, h->stream),
                "population upload");
+        FC_RC(guard_snapshot(h, h->stream, h->cur));
         FC_TRY(h, fc::launch_pops_in(h->q, h->storage, h->pop[h->cur], h->g, c0, nc, h->d_stage, layout_of(h),
                                      h->stream),
                "population write");
@@ -1102,6 +1146,194 @@ int fc_lbm_load_populations(fc_lbm* h, const float* in, size_t count) {
     FC_RC(aa_prime(h));
     // The loaded state is a post-step state: solid cells hold what was given.
     h->steps_since_reset = 0;
+    return wait_stream(h, kTransferTimeoutMs);
+}
+
+// ---- asynchronous field readback ----
+int fc_lbm_readback_field_async(fc_lbm* h, float* out, size_t count) {
+    FC_RC(check_ready(h));
+    if (!out || count != h->g.n * 4) return fail(h, FC_LBM_ERR_INVALID_ARG, "output must hold 4 floats per cell");
+    DeviceGuard dg(h->device);
+    if (h->rb_pending) FC_RC(fc_lbm_readback_wait(h, kTransferTimeoutMs));
+    if (!h->rb_stream) {
+        FC_TRY(h, cudaStreamCreateWithFlags(&h->rb_stream, cudaStreamNonBlocking), "create readback stream");
+        FC_TRY(h, cudaEventCreateWithFlags(&h->ev_snap, cudaEventDisableTiming), "create event");
+        FC_TRY(h, cudaEventCreateWithFlags(&h->ev_rb, cudaEventDisableTiming), "create event");
+    }
+    if (!h->d_snap) FC_TRY(h, cudaMalloc(&h->d_snap, h->g.n * 4 * sizeof(float)), "alloc readback snapshot");
+    // the snapshot reads the state every step queued so far leaves
+    FC_TRY(h, cudaEventRecord(h->ev_own, h->stream), "order readback");
+    FC_TRY(h, cudaStreamWaitEvent(h->rb_stream, h->ev_own, 0), "order readback");
+    FC_TRY(h, fc::launch_field(h->q, h->storage, h->pop[h->cur], h->d_solid, h->d_sdf, h->g, 0, h->g.n, h->d_snap,
+                               layout_of(h), h->rb_stream),
+           "snapshot field");
+    h->launches++;
+    FC_TRY(h, cudaEventRecord(h->ev_snap, h->rb_stream), "snapshot event");
+    h->snap_set = in_place(h) ? 0 : h->cur;
+    h->rb_pending = true;
+    FC_TRY(h, cudaMemcpyAsync(out, h->d_snap, h->g.n * 4 * sizeof(float), cudaMemcpyDeviceToHost, h->rb_stream),
+           "field download");
+    FC_TRY(h, cudaEventRecord(h->ev_rb, h->rb_stream), "readback event");
+    return FC_LBM_OK;
+}
+
+int fc_lbm_readback_wait(fc_lbm* h, int32_t timeout_ms) {
+    FC_RC(check_ready(h));
+    if (!h->rb_pending) return FC_LBM_OK;
+    DeviceGuard dg(h->device);
+    auto t0 = std::chrono::steady_clock::now();
+    int sleep_us = 5;
+    for (;;) {
+        const cudaError_t e = cudaEventQuery(h->ev_rb);
+        if (e == cudaSuccess) break;
+        if (e != cudaErrorNotReady) return cuda_fail(h, e, "readback failed");
+        if (timeout_ms >= 0 &&
+            std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count() >=
+                timeout_ms)
+            return fail(h, FC_LBM_ERR_TIMEOUT, "timed out waiting for the readback");
+        std::this_thread::sleep_for(std::chrono::microseconds(sleep_us));
+        sleep_us = std::min(sleep_us * 2, 500);
+    }
+    h->rb_pending = false;
+    h->snap_set = -1;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_alloc_pinned(size_t bytes, void** out) {
+    if (!out) return FC_LBM_ERR_INVALID_ARG;
+    *out = nullptr;
+    const cudaError_t e = cudaMallocHost(out, bytes);
+    if (e == cudaErrorMemoryAllocation) return FC_LBM_ERR_OUT_OF_MEMORY;
+    return e == cudaSuccess ? FC_LBM_OK : FC_LBM_ERR_CUDA;
+}
+
+int fc_lbm_free_pinned(void* p) {
+    if (!p) return FC_LBM_OK;
+    return cudaFreeHost(p) == cudaSuccess ? FC_LBM_OK : FC_LBM_ERR_CUDA;
+}
+
+// ---- smoke-trail particles (SmokeTrailSystem, FlowCraft/SmokeTrail.h:26-184) ----
+}  // extern "C"
+
+namespace {
+
+fc::SmokeParams smoke_params(const fc_lbm* h, int32_t confine_axis, int32_t confine_index) {
+    fc::SmokeParams sp{};
+    sp.ox = h->origin[0];
+    sp.oy = h->origin[1];
+    sp.oz = h->origin[2];
+    sp.cs = h->cell_size;
+    sp.confine_axis = confine_axis >= 0 && confine_axis <= 2 ? confine_axis : -1;
+    sp.confine_index = confine_index;
+    sp.seed = h->part_seed;
+    sp.counter = h->part_counter;
+    return sp;
+}
+
+// Draws one particle may take in one call: 8 attempts x 3 axes + 3 jitters.
+constexpr unsigned long long kDrawsPerCall = 32;
+
+}  // namespace
+
+extern "C" {
+
+int fc_lbm_particles_reset(fc_lbm* h, int32_t count, int32_t trail_length, uint64_t seed, int32_t confine_axis,
+                           int32_t confine_index) {
+    FC_RC(check_ready(h));
+    if (count < 0 || count > (1 << 26)) return fail(h, FC_LBM_ERR_INVALID_ARG, "particle count out of range");
+    DeviceGuard dg(h->device);
+    const int length = std::max(trail_length, 2);  // SmokeTrail.cpp:259
+    if ((long long)count * length > (1ll << 30)) return fail(h, FC_LBM_ERR_INVALID_ARG, "trails too long");
+    FC_RC(wait_stream(h, kTransferTimeoutMs));
+    dfree(h->parts.trail);
+    dfree(h->parts.head);
+    dfree(h->parts.len);
+    dfree(h->d_part_io);
+    dfree(h->d_part_lens);
+    h->parts = fc::ParticleSet{nullptr, nullptr, nullptr, count, length};
+    if (count > 0) {
+        FC_TRY(h, cudaMalloc(&h->parts.trail, (size_t)count * length * sizeof(float4)), "alloc particle trails");
+        FC_TRY(h, cudaMalloc(&h->parts.head, (size_t)count * sizeof(int)), "alloc particles");
+        FC_TRY(h, cudaMalloc(&h->parts.len, (size_t)count * sizeof(int)), "alloc particles");
+        FC_TRY(h, cudaMalloc(&h->d_part_io, (size_t)count * length * 3 * sizeof(float)), "alloc particle readout");
+        FC_TRY(h, cudaMalloc(&h->d_part_lens, (size_t)count * sizeof(int)), "alloc particle readout");
+    }
+    h->part_seed = seed;
+    h->part_counter = 0;
+    // Reset scatters over the whole domain (SmokeTrail.cpp:257-276)
+    FC_TRY(h, fc::launch_particles_scatter(h->d_solid, h->g, h->parts, smoke_params(h, confine_axis, confine_index),
+                                           h->stream),
+           "scatter particles");
+    h->part_counter += kDrawsPerCall;
+    h->launches++;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_particles_step(fc_lbm* h, int32_t reverse_flow, float mm_per_sec_per_lattice_unit, float dt_seconds,
+                          int32_t suspend_respawn, int32_t confine_axis, int32_t confine_index) {
+    FC_RC(check_ready(h));
+    if (!std::isfinite(mm_per_sec_per_lattice_unit) || !std::isfinite(dt_seconds)) return FC_LBM_ERR_INVALID_ARG;
+    if (h->parts.count == 0 || dt_seconds <= 0.0f) return FC_LBM_OK;  // SmokeTrail.cpp:281
+    DeviceGuard dg(h->device);
+    fc::SmokeParams sp = smoke_params(h, confine_axis, confine_index);
+    sp.reverse = reverse_flow != 0;
+    sp.suspend = suspend_respawn != 0;
+    const float dt = std::min(dt_seconds, 0.1f);  // kMaxDtSeconds, SmokeTrail.cpp:296-297
+    sp.scale = mm_per_sec_per_lattice_unit * dt;
+    FC_TRY(h, fc::launch_particles_step(h->q, h->storage, h->pop[h->cur], layout_of(h), h->d_solid, h->g, h->parts,
+                                        sp, h->stream),
+           "advect particles");
+    h->part_counter += kDrawsPerCall;
+    h->launches++;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_particles_scatter(fc_lbm* h, int32_t confine_axis, int32_t confine_index) {
+    FC_RC(check_ready(h));
+    DeviceGuard dg(h->device);
+    FC_TRY(h, fc::launch_particles_scatter(h->d_solid, h->g, h->parts, smoke_params(h, confine_axis, confine_index),
+                                           h->stream),
+           "scatter particles");
+    h->part_counter += kDrawsPerCall;
+    h->launches++;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_particles_shift_plane(fc_lbm* h, int32_t confine_axis, int32_t confine_index) {
+    FC_RC(check_ready(h));
+    if (confine_axis < 0 || confine_axis > 2) return FC_LBM_ERR_INVALID_ARG;
+    DeviceGuard dg(h->device);
+    FC_TRY(h, fc::launch_particles_shift(h->g, h->parts, smoke_params(h, confine_axis, confine_index), h->stream),
+           "shift particles");
+    h->launches++;
+    return FC_LBM_OK;
+}
+
+int fc_lbm_particles_read(fc_lbm* h, float* points, size_t points_count, int32_t* lens, size_t lens_count) {
+    FC_RC(check_ready(h));
+    const size_t np = (size_t)h->parts.count, nl = (size_t)h->parts.length;
+    if (!points || !lens || points_count != np * nl * 3 || lens_count != np) return FC_LBM_ERR_INVALID_ARG;
+    if (np == 0) return FC_LBM_OK;
+    DeviceGuard dg(h->device);
+    FC_TRY(h, fc::launch_particles_gather(h->parts, h->d_part_io, h->d_part_lens, h->stream), "gather trails");
+    h->launches++;
+    FC_TRY(h, cudaMemcpyAsync(points, h->d_part_io, np * nl * 3 * sizeof(float), cudaMemcpyDeviceToHost, h->stream),
+           "trail download");
+    FC_TRY(h, cudaMemcpyAsync(lens, h->d_part_lens, np * sizeof(int), cudaMemcpyDeviceToHost, h->stream),
+           "trail download");
+    return wait_stream(h, kTransferTimeoutMs);
+}
+
+int fc_lbm_particles_set(fc_lbm* h, const float* points, size_t points_count) {
+    FC_RC(check_ready(h));
+    const size_t np = (size_t)h->parts.count;
+    if (!points || points_count != np * 3) return FC_LBM_ERR_INVALID_ARG;
+    if (np == 0) return FC_LBM_OK;
+    DeviceGuard dg(h->device);
+    FC_TRY(h, cudaMemcpyAsync(h->d_part_io, points, np * 3 * sizeof(float), cudaMemcpyHostToDevice, h->stream),
+           "position upload");
+    FC_TRY(h, fc::launch_particles_set(h->parts, h->d_part_io, h->stream), "set particles");
+    h->launches++;
     return wait_stream(h, kTransferTimeoutMs);
 }
 
@@ -1266,6 +1498,7 @@ int batch_enter(fc_lbm_batch* b) {
     for (fc_lbm* h : b->m) {
         FB_TRY(b, cudaEventRecord(b->ev, h->stream), "member event");
         FB_TRY(b, cudaStreamWaitEvent(b->stream, b->ev, 0), "wait member");
+        if (h->rb_pending) FB_TRY(b, cudaStreamWaitEvent(b->stream, h->ev_snap, 0), "wait member readback snapshot");
     }
     return FC_LBM_OK;
 }

@@ -228,6 +228,31 @@ cudaError_t launch_aero(int q, int storage, const void* f, const uint8_t* solid,
                         float cell_size, float ox, float oy, float oz, double* partials, int blocks, double* result,
                         int layout, cudaStream_t s);
 
+// Smoke-trail particles (particles.cu): trails of `length` points per
+// particle in a ring (head = newest point, len = points kept, 0 = inactive).
+struct ParticleSet {
+    float4* trail;  // count * length points (x, y, z world, w unused)
+    int* head;
+    int* len;
+    int count, length;
+};
+struct SmokeParams {
+    float ox, oy, oz, cs;      // grid origin and cell size (world units)
+    int reverse;               // inlet face at x = nx-1
+    float scale;               // mm per second per lattice unit x dt (dt capped at 0.1 s)
+    int suspend;               // vanish instead of respawning
+    int confine_axis;          // -1 none, 0 / 1 / 2: the grid axis a plane fixes
+    int confine_index;
+    unsigned long long seed, counter;  // random draws: hash(seed, particle, counter + k)
+};
+cudaError_t launch_particles_step(int q, int storage, const void* f, int layout, const uint8_t* solid, const Geom& g,
+                                  const ParticleSet& ps, const SmokeParams& sp, cudaStream_t s);
+cudaError_t launch_particles_scatter(const uint8_t* solid, const Geom& g, const ParticleSet& ps, const SmokeParams& sp,
+                                     cudaStream_t s);
+cudaError_t launch_particles_shift(const Geom& g, const ParticleSet& ps, const SmokeParams& sp, cudaStream_t s);
+cudaError_t launch_particles_gather(const ParticleSet& ps, float* out, int* lens, cudaStream_t s);
+cudaError_t launch_particles_set(const ParticleSet& ps, const float* pos, cudaStream_t s);
+
 // Setup (geometry classification and boundary-list construction).
 // counts[0] += flagged (boundary-list) cells, counts[1] += bulk cells.
 cudaError_t launch_classify(int q, const uint8_t* solid, const Geom& g, uint8_t* flags, uint32_t* bulk_bits,

@@ -156,6 +156,16 @@ SIGNATURES = {
     "fc_lbm_wall_distance": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint8), _SZ]),
     "fc_lbm_closure_coverage": (ctypes.c_int, [_P, _U64P, _U64P]),
     "fc_lbm_layer_copy": (ctypes.c_int, [_P, _I32, _I32, _P, _I32, _P]),
+    "fc_lbm_readback_field_async": (ctypes.c_int, [_P, _P, _SZ]),
+    "fc_lbm_readback_wait": (ctypes.c_int, [_P, _I32]),
+    "fc_lbm_alloc_pinned": (ctypes.c_int, [_SZ, ctypes.POINTER(ctypes.c_void_p)]),
+    "fc_lbm_free_pinned": (ctypes.c_int, [_P]),
+    "fc_lbm_particles_reset": (ctypes.c_int, [_P, _I32, _I32, ctypes.c_uint64, _I32, _I32]),
+    "fc_lbm_particles_step": (ctypes.c_int, [_P, _I32, ctypes.c_float, ctypes.c_float, _I32, _I32, _I32]),
+    "fc_lbm_particles_scatter": (ctypes.c_int, [_P, _I32, _I32]),
+    "fc_lbm_particles_shift_plane": (ctypes.c_int, [_P, _I32, _I32]),
+    "fc_lbm_particles_read": (ctypes.c_int, [_P, _FP, _SZ, _I32P, _SZ]),
+    "fc_lbm_particles_set": (ctypes.c_int, [_P, _FP, _SZ]),
     "fc_lbm_batch_create": (ctypes.c_int, [ctypes.POINTER(_P), _I32, ctypes.POINTER(_P)]),
     "fc_lbm_batch_destroy": (None, [_P]),
     "fc_lbm_batch_last_error": (ctypes.c_char_p, [_P]),
@@ -483,6 +493,20 @@ class LbmSolver:
         return {"cells_in_range": int(a.value), "cell_fraction": a.value / max(n, 1),
                 "warps_with_mlp": int(b.value), "warp_fraction": b.value / max(warps, 1)}
 
+    def ReadbackFieldAsync(self, out) -> None:
+        """Starts a readback of the current field (4 floats per cell) into
+        `out` (a float32 array of 4*CellCount(), ideally from PinnedBuffer)
+        and returns; steps issued meanwhile overlap the copy. Keep `out`
+        alive until ReadbackWait()."""
+        if not isinstance(out, np.ndarray) or out.dtype != np.float32 or not out.flags.c_contiguous:
+            raise TypeError("out must be a contiguous float32 array of 4*CellCount()")
+        self._rb_out = out  # the copy lands here later
+        self._check(self._lib.fc_lbm_readback_field_async(self._h, out.ctypes.data, out.size), "ReadbackFieldAsync")
+
+    def ReadbackWait(self, timeout_ms: int = -1) -> None:
+        self._check(self._lib.fc_lbm_readback_wait(self._h, int(timeout_ms)), "ReadbackWait")
+        self._rb_out = None
+
     def LayerCopy(self, z: int, buffer_ptr: int, to_buffer: bool, next_set: bool = False, cmd=None) -> None:
         """Packs (to_buffer) or unpacks z-layer `z` of the current (or, with
         next_set, the in-progress step's output) population set to / from a
@@ -568,3 +592,31 @@ class LbmSolver:
         v = ctypes.c_uint64()
         self._lib.fc_lbm_launch_count(self._h, ctypes.byref(v))
         return v.value
+
+
+class PinnedBuffer:
+    """Page-locked host float32 array (fc_lbm_alloc_pinned), for
+    asynchronous readbacks. ``.array`` is the numpy view; free() or garbage
+    collection releases it."""
+
+    def __init__(self, count: int):
+        self._lib = load_library()
+        p = ctypes.c_void_p()
+        rc = self._lib.fc_lbm_alloc_pinned(int(count) * 4, ctypes.byref(p))
+        if rc != FC_LBM_OK:
+            raise LbmError(rc, "fc_lbm_alloc_pinned failed")
+        self._p = p.value
+        buf = (ctypes.c_float * int(count)).from_address(self._p)
+        self.array = np.ctypeslib.as_array(buf)
+
+    def free(self):
+        if getattr(self, "_p", None):
+            self.array = None
+            self._lib.fc_lbm_free_pinned(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

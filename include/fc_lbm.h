@@ -330,6 +330,64 @@ FC_LBM_API int fc_lbm_mlp_adam(float* params, const float* grad, float* m, float
  * (flowcraft_b200/shard.py) is built on it; no reference counterpart. */
 FC_LBM_API int fc_lbm_layer_copy(fc_lbm* h, int32_t z, int32_t next, void* buffer, int32_t to_buffer, void* stream);
 
+/* ---- Asynchronous field readback (overlapped with stepping) ----
+ * What FlowCraft's ReadbackFieldPacedGPU (main.cpp:2506-2555) does with
+ * adaptive blocking z-chunks so that a readback never stalls the solver:
+ * here one kernel snapshots the whole 4-float field (ReadbackField's layout)
+ * of the state every queued step leaves into a device buffer (16 bytes per
+ * cell, allocated on the first call) on a side stream, and the copy to
+ * `out` follows on that stream. The call returns at once; steps enqueued
+ * afterwards run while the copy is in flight and only the first one that
+ * overwrites the population set the snapshot reads waits for the snapshot
+ * kernel (not for the copy). `out` must stay valid until
+ * fc_lbm_readback_wait returns; page-locked memory (fc_lbm_alloc_pinned)
+ * lets the copy run asynchronously. One readback at a time: a second call
+ * first waits for the first. */
+FC_LBM_API int fc_lbm_readback_field_async(fc_lbm* h, float* out, size_t count);
+/* Waits (bounded, -1 = no limit) until the pending readback's copy has
+ * landed; FC_LBM_OK at once when none is pending. */
+FC_LBM_API int fc_lbm_readback_wait(fc_lbm* h, int32_t timeout_ms);
+/* Page-locked host memory for asynchronous readbacks. */
+FC_LBM_API int fc_lbm_alloc_pinned(size_t bytes, void** out);
+FC_LBM_API int fc_lbm_free_pinned(void* p);
+
+/* ---- Smoke-trail particles (SmokeTrailSystem, FlowCraft/SmokeTrail.h:26-184) ----
+ * Particles with short trails advected through the solver's own velocity,
+ * sampled on the device from the current populations (the velocity the field
+ * readback would report, trilinearly interpolated as SampleVelocityInterpolated
+ * does, SmokeTrail.cpp:69-116) instead of from a host copy of the field.
+ * Positions are world coordinates (VoxelGrid::CellCenter: grid x is world Y,
+ * grid y is world X). `confine_axis` < 0 means unconfined, else the grid axis
+ * (0 x, 1 y, 2 z) of a PlaneConfinement at `confine_index`. Random draws come
+ * from a counter-based hash of `seed` (the reference uses std::mt19937), so
+ * respawned particles land elsewhere than the reference's; the rules are the
+ * reference's. All calls are ordered on the solver's stream. */
+/* SmokeTrailSystem::Reset (SmokeTrail.cpp:257-276): `count` particles with
+ * trails of max(trail_length, 2) points, scattered over the domain (or plane).
+ * Allocates the particle buffers. */
+FC_LBM_API int fc_lbm_particles_reset(fc_lbm* h, int32_t count, int32_t trail_length, uint64_t seed,
+                                      int32_t confine_axis, int32_t confine_index);
+/* SmokeTrailSystem::Step (SmokeTrail.cpp:278-343): one advection of every
+ * particle by the current velocity x mm_per_sec_per_lattice_unit x
+ * min(dt_seconds, 0.1); a particle that left the grid or entered a solid cell
+ * respawns at the inlet face (or plane), or vanishes with suspend_respawn.
+ * dt_seconds <= 0 does nothing. Asynchronous. */
+FC_LBM_API int fc_lbm_particles_step(fc_lbm* h, int32_t reverse_flow, float mm_per_sec_per_lattice_unit,
+                                     float dt_seconds, int32_t suspend_respawn, int32_t confine_axis,
+                                     int32_t confine_index);
+/* SmokeTrailSystem::ScatterRandom (SmokeTrail.cpp:206-220). */
+FC_LBM_API int fc_lbm_particles_scatter(fc_lbm* h, int32_t confine_axis, int32_t confine_index);
+/* SmokeTrailSystem::ShiftPlane (SmokeTrail.cpp:222-255): every trail point onto
+ * the plane at confine_index along confine_axis (0..2). */
+FC_LBM_API int fc_lbm_particles_shift_plane(fc_lbm* h, int32_t confine_axis, int32_t confine_index);
+/* Every trail, oldest point first: points[(p * L + k) * 3 + 0..2] for
+ * k < lens[p], zeros after (L = the trail length of the last reset). Blocks. */
+FC_LBM_API int fc_lbm_particles_read(fc_lbm* h, float* points, size_t points_count, int32_t* lens,
+                                     size_t lens_count);
+/* Every particle to the single point points[p * 3 + 0..2] (world units),
+ * trail cleared. Blocks. */
+FC_LBM_API int fc_lbm_particles_set(fc_lbm* h, const float* points, size_t points_count);
+
 /* ---- Batches: many lattices stepped together (no reference counterpart) ----
  * For sweeps such as a set of angles of attack: the members (initialized
  * handles on one device, one lattice model and storage format, even nx, no

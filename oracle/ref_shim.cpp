@@ -185,3 +185,62 @@ void ref_aero_forces(int nx, int ny, int nz, float cell_size, const float* origi
 }
 
 }  // extern "C"
+
+// ---- SmokeTrailSystem::Step (FlowCraft/SmokeTrail.cpp:278-343) ----
+// The particle state is private to the class; the shim opens it (and only
+// it: the standard headers and FieldOverlay.h are already included above)
+// so a test can seed given positions, run the reference's own Step on a
+// field, and read the trails back.
+#include <random>
+#define private public
+#include "SmokeTrail.h"
+#undef private
+
+extern "C" {
+
+// Seeds `count` particles at pos[p*3 .. +2] (world units), runs `steps`
+// Step() calls on `field` (4 floats per cell), and writes every trail,
+// oldest point first, to out[(p * trail_length + k) * 3 + 0..2] with its
+// point count in lens[p]. confine_axis < 0: unconfined.
+int ref_smoke_step(int nx, int ny, int nz, float cell_size, const float* origin, const uint8_t* solid,
+                   const float* field, int count, int trail_length, const float* pos, int steps, int reverse,
+                   float mm_per_sec, float dt, int confine_axis, int confine_index, float* out, int* lens) {
+    VoxelGrid grid;
+    grid.nx = nx;
+    grid.ny = ny;
+    grid.nz = nz;
+    grid.cellSize = cell_size;
+    grid.origin = Vec3(origin[0], origin[1], origin[2]);
+    const size_t n = (size_t)nx * ny * nz;
+    grid.solid.assign(solid, solid + n);
+    std::vector<float> f(field, field + n * 4);
+    SmokeTrailSystem::PlaneConfinement conf{};
+    const SmokeTrailSystem::PlaneConfinement* cp = nullptr;
+    if (confine_axis >= 0) {
+        conf.axis = static_cast<SliceAxis>(confine_axis);
+        conf.index = confine_index;
+        cp = &conf;
+    }
+    SmokeTrailSystem sys;
+    sys.Reset(grid, reverse != 0, count, trail_length, cp);
+    for (int p = 0; p < count; ++p) {
+        sys.particles_[(size_t)p].trail.clear();
+        sys.particles_[(size_t)p].trail.push_back(Vec3(pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]));
+    }
+    for (int s = 0; s < steps; ++s) sys.Step(grid, f, reverse != 0, mm_per_sec, dt, false, cp);
+    for (int p = 0; p < count; ++p) {
+        const auto& t = sys.particles_[(size_t)p].trail;
+        lens[p] = (int)t.size();
+        for (int k = 0; k < trail_length; ++k) {
+            float* o = out + ((size_t)p * trail_length + k) * 3;
+            if (k < (int)t.size()) {
+                o[0] = t[(size_t)k].x, o[1] = t[(size_t)k].y, o[2] = t[(size_t)k].z;
+            } else {
+                o[0] = o[1] = o[2] = 0.0f;
+            }
+        }
+    }
+    return 0;
+}
+
+}  // extern "C"
