@@ -396,6 +396,7 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned(const 
     using T = typename S::T;
     __shared__ uint32_t s_in[kBulkRows][32 * 8];
     __shared__ float2 s_out[kBulkRows][32];
+    __shared__ float2 s_mo[kBulkRows][12][32];  // the relaxation's moments while the MLP runs
     const int y = blockIdx.y * kBulkRows + threadIdx.y;
     const int z = z0 + blockIdx.z;
     if (y >= g.ny) return;  // the whole warp: one row
@@ -474,38 +475,42 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned(const 
     }
     // A cell outside the training range takes the Smagorinsky value, so a
     // warp with no cell in range has no use for the MLP and skips it (the
-    // result is the same).
-    float2 nu = make_float2(0.0f, 0.0f);
+    // result is the same): it relaxes with Smagorinsky and is done.
     const unsigned need = __ballot_sync(0xffffffffu, la || lb);
-    if (need) {
-        // row tiles of the MLP (8 lanes each) with a cell in range
-        const unsigned tiles = ((need & 0xffu) ? 1u : 0u) | ((need & 0xff00u) ? 2u : 0u) |
-                               ((need & 0xff0000u) ? 4u : 0u) | ((need & 0xff000000u) ? 8u : 0u);
-        // both cells' wall distances in one aligned load (x and nx are even)
-        const unsigned wd = pair ? (unsigned)__ldg(reinterpret_cast<const unsigned short*>(cl.wall + c)) : 0xffffu;
-        uint32_t* in = &s_in[threadIdx.y][threadIdx.x * 8];
-        closure_pack_inputs(cl, xa0, xa1, xa2, (float)(wd & 0xffu) * 0.0625f, in);
-        closure_pack_inputs(cl, xb0, xb1, xb2, (float)(wd >> 8) * 0.0625f, in + 4);
-        __syncwarp();
-        nu = closure_warp_mlp(cl.frag, s_in[threadIdx.y], s_out[threadIdx.y], tiles);
+    if (!need) {
+        if (!pair) return;
+        relax2<Q>(v, mo, make_float2(sga, sgb));
+        if (bad) atomicOr(diverged, 1);
+        store_pair<Q, S>(pp, c, v, pair);
+        return;
     }
+    // The MLP path. The moments the relaxation needs wait in shared memory
+    // (this warp's own slice) while the MLP holds the registers.
+    float2* sm = &s_mo[threadIdx.y][0][threadIdx.x];
+    sm[0 * 32] = mo.rho, sm[1 * 32] = mo.drho, sm[2 * 32] = mo.u2, sm[3 * 32] = mo.ux;
+    sm[4 * 32] = mo.uy, sm[5 * 32] = mo.uz, sm[6 * 32] = mo.pxx, sm[7 * 32] = mo.pyy;
+    sm[8 * 32] = mo.pzz, sm[9 * 32] = mo.pxy, sm[10 * 32] = mo.pxz, sm[11 * 32] = mo.pyz;
+    // row tiles of the MLP (8 lanes each) with a cell in range
+    const unsigned tiles = ((need & 0xffu) ? 1u : 0u) | ((need & 0xff00u) ? 2u : 0u) |
+                           ((need & 0xff0000u) ? 4u : 0u) | ((need & 0xff000000u) ? 8u : 0u);
+    // both cells' wall distances in one aligned load (x and nx are even)
+    const unsigned wd = pair ? (unsigned)__ldg(reinterpret_cast<const unsigned short*>(cl.wall + c)) : 0xffffu;
+    uint32_t* in = &s_in[threadIdx.y][threadIdx.x * 8];
+    closure_pack_inputs(cl, xa0, xa1, xa2, (float)(wd & 0xffu) * 0.0625f, in);
+    closure_pack_inputs(cl, xb0, xb1, xb2, (float)(wd >> 8) * 0.0625f, in + 4);
+    __syncwarp();
+    const float2 nu = closure_warp_mlp(cl.frag, s_in[threadIdx.y], s_out[threadIdx.y], tiles);
     if (!pair) return;
+    Mom2 mr;
+    mr.rho = sm[0 * 32], mr.drho = sm[1 * 32], mr.u2 = sm[2 * 32], mr.ux = sm[3 * 32];
+    mr.uy = sm[4 * 32], mr.uz = sm[5 * 32], mr.pxx = sm[6 * 32], mr.pyy = sm[7 * 32];
+    mr.pzz = sm[8 * 32], mr.pxy = sm[9 * 32], mr.pxz = sm[10 * 32], mr.pyz = sm[11 * 32];
     float2 gr;
     gr.x = la ? (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.x, p.tau))) * 4.5f : sga;
     gr.y = lb ? (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.y, p.tau))) * 4.5f : sgb;
-    relax2<Q>(v, mo, gr);
+    relax2<Q>(v, mr, gr);
     if (bad) atomicOr(diverged, 1);
-    static_for<0, Q>([&](auto I) {
-        constexpr int i = decltype(I)::value;
-        T* dst = static_cast<T*>(pp.dst[i]);
-        const typename S::T2 hv = S::pack2(v[i].x, v[i].y);
-        if (pair == 3u) {
-            *reinterpret_cast<typename S::T2*>(dst + c) = hv;
-        } else {
-            if (va) dst[c] = hv.x;
-            if (vb) dst[c + 1u] = hv.y;
-        }
-    });
+    store_pair<Q, S>(pp, c, v, pair);
 }
 
 // The closure's inputs and nu_t for every cell of the current population set
