@@ -99,10 +99,14 @@ __device__ __forceinline__ float4 fluid_moments(const typename S::T* __restrict_
     return make_float4(rho, ux, uy, uz);
 }
 
-template <int Q, class S>
+template <int Q, class S, int Lay>
 __global__ void __launch_bounds__(256) k_field(const typename S::T* __restrict__ f, const uint8_t* __restrict__ solid,
                                                 const float* __restrict__ sdf, Geom g, size_t cell0, size_t cells,
-                                                float4* __restrict__ out, int layout) {
+                                                float4* __restrict__ out, int layout_in) {
+    // the layout is a compile-time constant, so every slot folds to its
+    // formula (plane * n + c for plane-major states)
+    const int layout = Lay;
+    (void)layout_in;
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= cells) return;
     const size_t c = cell0 + k;
@@ -114,17 +118,24 @@ __global__ void __launch_bounds__(256) k_field(const typename S::T* __restrict__
                       : fluid_moments<Q, S>(f, g, c, x, y, z, layout);
 }
 
-template <int Q, class S>
+template <int Q, class S, int Lay>
 __global__ void k_pops_out(const typename S::T* __restrict__ f, const uint8_t* __restrict__ solid,
                            int solid_is_weight, Geom g, size_t cell0, size_t cells, float* __restrict__ out,
-                           int layout) {
+                           int layout_in) {
+    // the layout is a compile-time constant, so every slot folds to its
+    // formula (plane * n + c for plane-major states)
+    const int layout = Lay;
+    (void)layout_in;
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= cells) return;
     const size_t c = cell0 + k;
-    const int z = (int)(c / (size_t)g.nxy);
-    const size_t rem = c - (size_t)z * g.nxy;
-    const int y = (int)(rem / g.nx);
-    const int x = (int)(rem - (size_t)y * g.nx);
+    int x = 0, y = 0, z = 0;
+    if (layout != kLayoutPlanes) {  // the plane-major slot needs no coordinates
+        z = (int)(c / (size_t)g.nxy);
+        const size_t rem = c - (size_t)z * g.nxy;
+        y = (int)(rem / g.nx);
+        x = (int)(rem - (size_t)y * g.nx);
+    }
     const bool sw = solid_is_weight && solid[c];
     static_for<0, Q>([&](auto I) {
         constexpr int i = decltype(I)::value;
@@ -132,16 +143,23 @@ __global__ void k_pops_out(const typename S::T* __restrict__ f, const uint8_t* _
     });
 }
 
-template <int Q, class S>
+template <int Q, class S, int Lay>
 __global__ void k_pops_in(typename S::T* __restrict__ f, Geom g, size_t cell0, size_t cells,
-                          const float* __restrict__ in, int layout) {
+                          const float* __restrict__ in, int layout_in) {
+    // the layout is a compile-time constant, so every slot folds to its
+    // formula (plane * n + c for plane-major states)
+    const int layout = Lay;
+    (void)layout_in;
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= cells) return;
     const size_t c = cell0 + k;
-    const int z = (int)(c / (size_t)g.nxy);
-    const size_t rem = c - (size_t)z * g.nxy;
-    const int y = (int)(rem / g.nx);
-    const int x = (int)(rem - (size_t)y * g.nx);
+    int x = 0, y = 0, z = 0;
+    if (layout != kLayoutPlanes) {
+        z = (int)(c / (size_t)g.nxy);
+        const size_t rem = c - (size_t)z * g.nxy;
+        y = (int)(rem / g.nx);
+        x = (int)(rem - (size_t)y * g.nx);
+    }
     static_for<0, Q>([&](auto I) {
         constexpr int i = decltype(I)::value;
         f[pop_slot<Q, i>(c, x, y, z, g, layout)] = S::enc(in[(size_t)i * cells + k], Lattice<Q>::w(i));
@@ -211,18 +229,28 @@ __device__ __forceinline__ void stat_block_reduce(StatAcc& acc, double* out) {
     }
 }
 
-template <int Q, class S>
+template <int Q, class S, int Lay>
 __global__ void __launch_bounds__(kStatsThreads) k_stats(const typename S::T* __restrict__ f,
                                                          const uint8_t* __restrict__ solid,
                                                          const float* __restrict__ sdf, Geom g,
-                                                         double* __restrict__ partials, int layout) {
+                                                         double* __restrict__ partials, int layout_in) {
+    // the layout is a compile-time constant, so every slot folds to its
+    // formula (plane * n + c for plane-major states)
+    const int layout = Lay;
+    (void)layout_in;
     StatAcc acc;
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < g.n; c += (size_t)gridDim.x * blockDim.x) {
-        const int z = (int)(c / (size_t)g.nxy);
-        const size_t rem = c - (size_t)z * g.nxy;
-        const int y = (int)(rem / g.nx);
-        const int x = (int)(rem - (size_t)y * g.nx);
-        if (solid[c]) {
+        const bool sol = solid[c];
+        // cell coordinates only where they are used: the solid-cell force and
+        // the in-place layouts (the plane-major slot is plane * n + c)
+        int x = 0, y = 0, z = 0;
+        if (sol || layout != kLayoutPlanes) {
+            z = (int)(c / (size_t)g.nxy);
+            const size_t rem = c - (size_t)z * g.nxy;
+            y = (int)(rem / g.nx);
+            x = (int)(rem - (size_t)y * g.nx);
+        }
+        if (sol) {
             const float4 v = solid_force<Q, S>(f, solid, sdf, g, x, y, z, c, layout);
             if (isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(v.w)) {
                 acc.fx += (double)v.y;
@@ -312,12 +340,16 @@ __device__ void aero_block_reduce(double* a, double* out) {
     }
 }
 
-template <int Q, class S>
+template <int Q, class S, int Lay>
 __global__ void __launch_bounds__(kStatsThreads) k_aero(const typename S::T* __restrict__ f,
                                                         const uint8_t* __restrict__ solid,
                                                         const float* __restrict__ sdf, Geom g, float cs, float ox,
                                                         float oy, float oz, double* __restrict__ partials,
-                                                        int layout) {
+                                                        int layout_in) {
+    // the layout is a compile-time constant, so every slot folds to its
+    // formula (plane * n + c for plane-major states)
+    const int layout = Lay;
+    (void)layout_in;
     double a[kAeroSlots];
     aero_init(a);
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < g.n; c += (size_t)gridDim.x * blockDim.x) {
@@ -441,12 +473,23 @@ int stats_blocks(const Geom& g) {
     return (int)(want < 1 ? 1 : (want > cap ? cap : want));
 }
 
+// Launches KERNEL<Q, S, layout> for the run-time `layout` (PopLayout).
+#define FC_LAYOUT_LAUNCH(KERNEL, GRID, BLOCK, ...)                                        \
+    do {                                                                                  \
+        if (layout == kLayoutAAEven)                                                      \
+            KERNEL<Q, S, kLayoutAAEven><<<GRID, BLOCK, 0, s>>>(__VA_ARGS__);              \
+        else if (layout == kLayoutAAOdd)                                                  \
+            KERNEL<Q, S, kLayoutAAOdd><<<GRID, BLOCK, 0, s>>>(__VA_ARGS__);               \
+        else                                                                              \
+            KERNEL<Q, S, kLayoutPlanes><<<GRID, BLOCK, 0, s>>>(__VA_ARGS__);              \
+    } while (0)
+
 template <int Q, class S>
 static cudaError_t field_t(const void* f, const uint8_t* solid, const float* sdf, const Geom& g, size_t cell0,
                            size_t cells, float* out, int layout, cudaStream_t s) {
     if (cells == 0) return cudaSuccess;
-    k_field<Q, S><<<(unsigned)((cells + 255) / 256), 256, 0, s>>>((const typename S::T*)f, solid, sdf, g, cell0, cells,
-                                                                  (float4*)out, layout);
+    FC_LAYOUT_LAUNCH(k_field, (unsigned)((cells + 255) / 256), 256, (const typename S::T*)f, solid, sdf, g, cell0,
+                     cells, (float4*)out, layout);
     return cudaGetLastError();
 }
 
@@ -454,8 +497,8 @@ template <int Q, class S>
 static cudaError_t pops_out_t(const void* f, const uint8_t* solid, int sw, const Geom& g, size_t cell0, size_t cells,
                               float* out, int layout, cudaStream_t s) {
     if (cells == 0) return cudaSuccess;
-    k_pops_out<Q, S><<<(unsigned)((cells + 255) / 256), 256, 0, s>>>((const typename S::T*)f, solid, sw, g, cell0,
-                                                                     cells, out, layout);
+    FC_LAYOUT_LAUNCH(k_pops_out, (unsigned)((cells + 255) / 256), 256, (const typename S::T*)f, solid, sw, g, cell0,
+                     cells, out, layout);
     return cudaGetLastError();
 }
 
@@ -463,14 +506,14 @@ template <int Q, class S>
 static cudaError_t pops_in_t(void* f, const Geom& g, size_t cell0, size_t cells, const float* in, int layout,
                              cudaStream_t s) {
     if (cells == 0) return cudaSuccess;
-    k_pops_in<Q, S><<<(unsigned)((cells + 255) / 256), 256, 0, s>>>((typename S::T*)f, g, cell0, cells, in, layout);
+    FC_LAYOUT_LAUNCH(k_pops_in, (unsigned)((cells + 255) / 256), 256, (typename S::T*)f, g, cell0, cells, in, layout);
     return cudaGetLastError();
 }
 
 template <int Q, class S>
 static cudaError_t stats_t(const void* f, const uint8_t* solid, const float* sdf, const Geom& g, double* partials,
                            int blocks, double* result, int layout, cudaStream_t s) {
-    k_stats<Q, S><<<blocks, kStatsThreads, 0, s>>>((const typename S::T*)f, solid, sdf, g, partials, layout);
+    FC_LAYOUT_LAUNCH(k_stats, blocks, kStatsThreads, (const typename S::T*)f, solid, sdf, g, partials, layout);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_stats_final<<<1, kStatsThreads, 0, s>>>(partials, blocks, result);
@@ -515,8 +558,8 @@ template <int Q, class S>
 static cudaError_t aero_t(const void* f, const uint8_t* solid, const float* sdf, const Geom& g, float cs, float ox,
                           float oy, float oz, double* partials, int blocks, double* result, int layout,
                           cudaStream_t s) {
-    k_aero<Q, S><<<blocks, kStatsThreads, 0, s>>>((const typename S::T*)f, solid, sdf, g, cs, ox, oy, oz, partials,
-                                                  layout);
+    FC_LAYOUT_LAUNCH(k_aero, blocks, kStatsThreads, (const typename S::T*)f, solid, sdf, g, cs, ox, oy, oz, partials,
+                     layout);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_aero_final<<<1, kStatsThreads, 0, s>>>(partials, blocks, solid, g, cs, ox, oy, oz, result);

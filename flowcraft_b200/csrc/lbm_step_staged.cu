@@ -287,7 +287,7 @@ static cudaError_t tiles_t(const void* fin, void* fout, const uint32_t* bits, co
         const cuuint32_t box[2] = {(cuuint32_t)St::kCols, (cuuint32_t)kTileRows};
         const cuuint32_t estr[2] = {1, 1};
         if (encode(&map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, const_cast<void*>(fin), dims, strides, box, estr,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return cudaErrorInvalidValue;
 
