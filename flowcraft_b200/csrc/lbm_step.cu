@@ -110,80 +110,6 @@ __global__ void __launch_bounds__(32 * kBulkRows) k_bulk_interior(const typename
     bulk_cell<Q, S, false>(fin, fout, g, p, x, y, z, c, diverged);
 }
 
-// Interior, two x-adjacent cells per thread (lattices with even nx): a warp
-// covers 64 cells of a row starting at x = 32 + 64*blockIdx.x, so every pair
-// starts on an even cell index. The directions with e_x = 0 read both cells
-// of a pair with one aligned 2-element load, every store is one 2-element
-// store, and both cells share each address. Per direction the source pointer
-// fin + i*n - offset_i is the same for every thread, so an access costs one
-// index-times-stride from a uniform base. Pairs with one bulk cell (next to a
-// wall) fall back to the one-cell path for that cell.
-template <int Q, class S>
-__global__ void __launch_bounds__(32 * kBulkRows) k_bulk_interior2(const typename S::T* __restrict__ fin,
-                                                                    typename S::T* __restrict__ fout,
-                                                                    const uint32_t* __restrict__ bulk_bits, Geom g,
-                                                                    StepParams p, PlanePtrs pp, int z0,
-                                                                    int* __restrict__ diverged) {
-    using L = Lattice<Q>;
-    using T = typename S::T;
-    const int w0 = 1 + 2 * blockIdx.x;  // first 32-cell chunk of this warp's 64 cells
-    const int y = 1 + blockIdx.y * kBulkRows + threadIdx.y;
-    const int z = z0 + blockIdx.z;
-    if (y >= g.ny - 1) return;
-    const size_t row = (size_t)z * g.ny + y;
-    const int k = 2 * threadIdx.x;  // 0..62 within the 64 cells
-    const int w = w0 + (k >> 5);
-    const uint32_t bits = w <= g.wpr - 2 ? __ldg(bulk_bits + row * g.wpr + w) : 0u;
-    const unsigned pair = (bits >> (k & 31)) & 3u;
-    if (!pair) return;
-    const int x = w0 * 32 + k;
-    const uint32_t c = (uint32_t)(row * g.nx + x);
-    if (pair != 3u) {  // only one of the two cells is a bulk cell
-        const uint32_t cc = pair == 1u ? c : c + 1u;
-        bulk_cell<Q, S, false>(fin, fout, g, p, x + (pair == 1u ? 0 : 1), y, z, cc, diverged);
-        return;
-    }
-    // both cells of the pair in one float2 per direction (cell x in .x)
-    float2 v[Q];
-    static_for<0, Q>([&](auto I) {
-        constexpr int i = decltype(I)::value;
-        const T* src = static_cast<const T*>(pp.src[i]);
-        if constexpr (S::kExact) {
-            v[i] = L::ex(i) == 0 ? S::dec2(S::ld2(src + c), L::w(i))
-                                 : make_float2(S::dec(S::ld(src + c), L::w(i)), S::dec(S::ld(src + c + 1u), L::w(i)));
-        } else {  // 16-bit offsets: collide on the stored representation
-            v[i] = L::ex(i) == 0 ? S::raw2(S::ld2(src + c))
-                                 : make_float2(S::raw(S::ld(src + c)), S::raw(S::ld(src + c + 1u)));
-        }
-    });
-    bool bad;
-    if constexpr (S::kExact) {  // bit-exact path: the scalar reference-order collision per cell
-        float a[Q], b[Q];
-        static_for<0, Q>([&](auto I) {
-            constexpr int i = decltype(I)::value;
-            a[i] = v[i].x;
-            b[i] = v[i].y;
-        });
-        bad = collide_regularized<Q>(a, p.tau, p.cs);
-        bad |= collide_regularized<Q>(b, p.tau, p.cs);
-        static_for<0, Q>([&](auto I) {
-            constexpr int i = decltype(I)::value;
-            v[i] = make_float2(a[i], b[i]);
-        });
-    } else {
-        bad = collide_offsets2<Q>(v, p.tau, p.cs) != 0u;
-    }
-    if (bad) atomicOr(diverged, 1);
-    static_for<0, Q>([&](auto I) {
-        constexpr int i = decltype(I)::value;
-        T* dst = static_cast<T*>(pp.dst[i]);
-        if constexpr (S::kExact)
-            *reinterpret_cast<typename S::T2*>(dst + c) = S::enc2(v[i].x, v[i].y, L::w(i));
-        else
-            *reinterpret_cast<typename S::T2*>(dst + c) = S::pack2(v[i].x, v[i].y);
-    });
-}
-
 // One inlet or outlet cell (x = 0 or x = nx-1, fluid): equilibrium at the
 // inlet (LbmReference.cpp:269-273); at the outlet, equilibrium from the
 // upstream neighbour's fIn moments with rho relaxed toward 1
