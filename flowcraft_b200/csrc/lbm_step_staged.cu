@@ -5,15 +5,22 @@
 // A tile is 8 rows x 64 cells of one z layer: rows y0 .. y0+7 off the Y
 // faces, one 64-cell chunk off the row ends, a layer off the Z faces (the
 // interior warps of k_bulk_pairs). For direction i the tile pulls rows
-// (y0 - e_y .. y0 - e_y + 7) of layer z - e_z in plane i, cells
-// [x0 - 8, x0 + 72): one 2D tensor copy of an 80 x 8 box, 16-byte aligned in
-// x, so a tile's Q sources arrive as Q copies (one per direction) instead of
-// Q x 8 x 2 element loads per lane pair.
+// (y0 - e_y .. y0 - e_y + 7) of layer z - e_z in plane i:
+//   * cells [x0, x0 + 64) as one 2D tensor copy of a 64 x 8 box, whose rows
+//     start on 128-byte boundaries (whole 32-byte sectors, nothing shared
+//     with the neighbouring tiles);
+//   * for e_x = +1 also cell x0 - 1, and for e_x = -1 cell x0 + 64, as an
+//     8 x 8 box of the same rows (16 bytes per row, the smallest tensor copy
+//     that keeps x 16-byte aligned): [x0 - 8, x0) or [x0 + 64, x0 + 72),
+//     both inside the row since the chunk is not the first or last.
+// A D3Q19 or D3Q15 tile's sources arrive as Q main copies and 10 halo copies
+// instead of Q x 8 x 2 element loads per lane pair.
 //
 // Each block is a pipeline of kTileStages tiles:
-//   * a producer warp (one elected lane) waits until the 8 consumer warps
+//   * a producer warp (its lane 0) waits until the 8 consumer warps
 //     have released a stage (the "empty" barrier, 8 arrivals), arms the
-//     stage's "full" barrier with the byte count, and issues the Q copies;
+//     stage's "full" barrier with the byte count, and issues the tile's
+//     Q + 10 copies;
 //   * consumer warp r computes row y0 + r of the tile: each lane takes the
 //     cell pair (x, x+1), reads its Q values from shared memory at the e_x
 //     shift, collides exactly as k_bulk_pairs does (the pair collision for
@@ -87,15 +94,6 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
-// e_y + 1 and e_z + 1 of every direction in 2-bit fields (run-time index).
-template <int Q>
-__host__ __device__ constexpr unsigned long long packed_e(bool z) {
-    unsigned long long v = 0;
-    for (int i = 0; i < Q; ++i)
-        v |= (unsigned long long)((z ? Lattice<Q>::ez(i) : Lattice<Q>::ey(i)) + 1) << (2 * i);
-    return v;
-}
-
 // Work decomposition of one launch: tile t -> (z, y0, chunk).
 struct TilePlan {
     unsigned long long tiles;
@@ -104,12 +102,36 @@ struct TilePlan {
     int yblocks;  // 8-row blocks over the interior rows 1 .. ny-2
 };
 
+// e_x + 1, e_y + 1 or e_z + 1 of every direction in 2-bit fields (axis 0, 1,
+// 2), for run-time indexing.
+template <int Q>
+__host__ __device__ constexpr unsigned long long packed_e(int axis) {
+    unsigned long long v = 0;
+    for (int i = 0; i < Q; ++i) {
+        const int e = axis == 0 ? Lattice<Q>::ex(i) : axis == 1 ? Lattice<Q>::ey(i) : Lattice<Q>::ez(i);
+        v |= (unsigned long long)(e + 1) << (2 * i);
+    }
+    return v;
+}
+
+// Halo slot of direction i among the directions with e_x != 0, in order.
+template <int Q>
+__host__ __device__ constexpr int halo_slot(int i) {
+    int h = 0;
+    for (int j = 0; j < i; ++j) h += Lattice<Q>::ex(j) != 0;
+    return h;
+}
+
 template <int Q, class S>
 struct TileStaging {
-    static constexpr int kH = 16 / S::kBytes;  // halo elements per side
-    static constexpr int kCols = 64 + 2 * kH;
-    static constexpr uint32_t kBoxBytes = (uint32_t)kCols * kTileRows * S::kBytes;  // a multiple of 128
-    static constexpr uint32_t kStageBytes = Q * kBoxBytes;
+    static constexpr int kCols = 64;                 // main box width
+    static constexpr int kHaloCols = 16 / S::kBytes;  // halo box width (16 bytes)
+    static constexpr int kHalos = halo_slot<Q>(Q);   // directions with e_x != 0
+    static constexpr int kMain = kCols * kTileRows;  // elements per main box
+    static constexpr int kHalo = kHaloCols * kTileRows;
+    static constexpr uint32_t kMainBytes = (uint32_t)kMain * S::kBytes;  // a multiple of 128
+    static constexpr uint32_t kHaloBytes = (uint32_t)kHalo * S::kBytes;  // 128
+    static constexpr uint32_t kStageBytes = Q * kMainBytes + kHalos * kHaloBytes;
     static constexpr size_t kSmem = (size_t)kTileStages * kStageBytes + 128;  // + alignment slack
 };
 
@@ -117,6 +139,7 @@ struct TileStaging {
 
 template <int Q, class S>
 __global__ void __launch_bounds__(kTileThreads, kTileBlocksPerSm) k_bulk_tiles(const __grid_constant__ CUtensorMap map,
+                                                                              const __grid_constant__ CUtensorMap halo,
                                                                               const uint32_t* __restrict__ bulk_bits,
                                                                               Geom g, StepParams p, PlanePtrs pp,
                                                                               TilePlan plan,
@@ -125,6 +148,7 @@ __global__ void __launch_bounds__(kTileThreads, kTileBlocksPerSm) k_bulk_tiles(c
     using T = typename S::T;
     using T2 = typename S::T2;
     using St = TileStaging<Q, S>;
+    constexpr int kStage = St::kStageBytes / sizeof(T);  // elements per stage
     extern __shared__ unsigned char smem_raw[];
     __shared__ __align__(8) unsigned long long full[kTileStages], empty[kTileStages];
     T* stages = reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
@@ -150,7 +174,7 @@ __global__ void __launch_bounds__(kTileThreads, kTileBlocksPerSm) k_bulk_tiles(c
 
     if (warp == kTileRows) {  // producer
         if (lane != 0) return;
-        constexpr unsigned long long kEy = packed_e<Q>(false), kEz = packed_e<Q>(true);
+        constexpr unsigned long long kEx = packed_e<Q>(0), kEy = packed_e<Q>(1), kEz = packed_e<Q>(2);
         const long long layer_rows = (long long)g.ny * g.nz;
         unsigned long long k = 0;
         for (; k < count; ++k) {
@@ -163,11 +187,20 @@ __global__ void __launch_bounds__(kTileThreads, kTileBlocksPerSm) k_bulk_tiles(c
             tile_of(k, z, y0, cx);
             const uint32_t bar = smem_u32(&full[s]);
             mbar_expect_tx(bar, St::kStageBytes);
-            const uint32_t dst = smem_u32(stages + (size_t)s * (St::kStageBytes / sizeof(T)));
+            const uint32_t dst = smem_u32(stages + (size_t)s * kStage);
+            const uint32_t dst_halo = dst + Q * St::kMainBytes;
+            const int x0 = 64 * cx;
+            int h = 0;
             for (int i = 0; i < Q; ++i) {
+                const int ex = (int)((kEx >> (2 * i)) & 3ull) - 1;
                 const int ey = (int)((kEy >> (2 * i)) & 3ull) - 1, ez = (int)((kEz >> (2 * i)) & 3ull) - 1;
-                const long long row = (long long)i * layer_rows + (long long)(z - ez) * g.ny + (y0 - ey);
-                tma_load_2d(dst + (uint32_t)i * St::kBoxBytes, &map, 64 * cx - St::kH, (int)row, bar);
+                const int row = (int)((long long)i * layer_rows + (long long)(z - ez) * g.ny + (y0 - ey));
+                tma_load_2d(dst + (uint32_t)i * St::kMainBytes, &map, x0, row, bar);
+                if (ex != 0) {
+                    tma_load_2d(dst_halo + (uint32_t)h * St::kHaloBytes, &halo, ex > 0 ? x0 - St::kHaloCols : x0 + 64,
+                                row, bar);
+                    ++h;
+                }
             }
         }
         // copies still in flight land in this block's stages: wait for them (bounded)
@@ -180,7 +213,23 @@ __global__ void __launch_bounds__(kTileThreads, kTileBlocksPerSm) k_bulk_tiles(c
 
     // consumer warp `warp`: row y0 + warp of every tile
     const int kk = 2 * lane;
-    constexpr int kBox = St::kBoxBytes / sizeof(T);
+    // source of cell kk + j - e_x, j in {0, 1}, of direction i: the main box,
+    // or for the row's first / last cell the halo box (its last / first column)
+    auto src = [&](const T* st, auto I, int j) -> const T* {
+        constexpr int i = decltype(I)::value;
+        constexpr int ex = L::ex(i);
+        const T* main = st + i * St::kMain + warp * St::kCols;
+        if constexpr (ex == 0) {
+            return main + kk + j;
+        } else {
+            const T* hal = st + Q * St::kMain + halo_slot<Q>(i) * St::kHalo + warp * St::kHaloCols;
+            const int x = kk + j - ex;  // -1 .. 64
+            if constexpr (ex > 0)
+                return x < 0 ? hal + (St::kHaloCols - 1) : main + x;
+            else
+                return x >= 64 ? hal : main + x;
+        }
+    };
     for (unsigned long long k = 0; k < count; ++k) {
         const int s = (int)(k % kTileStages);
         if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((k / kTileStages) & 1))) {
@@ -191,27 +240,28 @@ __global__ void __launch_bounds__(kTileThreads, kTileBlocksPerSm) k_bulk_tiles(c
         tile_of(k, z, y0, cx);
         const int y = y0 + warp;
         if (y <= g.ny - 2) {
-            const T* sm = stages + (size_t)s * (St::kStageBytes / sizeof(T)) + warp * St::kCols + St::kH + kk;
+            const T* st = stages + (size_t)s * kStage;
             const size_t row = (size_t)z * g.ny + y;
             const uint32_t bits = __ldg(bulk_bits + row * g.wpr + 2 * cx + (kk >> 5));
             const unsigned pair = (bits >> (kk & 31)) & 3u;
             const uint32_t c = (uint32_t)(row * g.nx + 64 * cx + kk);
+            T* const fout = static_cast<T*>(pp.dst[0]);
             if (pair == 3u) {
                 float2 v[Q];
                 static_for<0, Q>([&](auto I) {
                     constexpr int i = decltype(I)::value;
-                    const T* r = sm + (i * kBox - L::ex(i));
                     if constexpr (L::ex(i) == 0) {
-                        const T2 h = *reinterpret_cast<const T2*>(r);
+                        const T2 h = *reinterpret_cast<const T2*>(src(st, I, 0));
                         if constexpr (S::kExact)
                             v[i] = S::dec2(h, L::w(i));
                         else
                             v[i] = S::raw2(h);
                     } else {
+                        const T a = *src(st, I, 0), b = *src(st, I, 1);
                         if constexpr (S::kExact)
-                            v[i] = make_float2(S::dec(r[0], L::w(i)), S::dec(r[1], L::w(i)));
+                            v[i] = make_float2(S::dec(a, L::w(i)), S::dec(b, L::w(i)));
                         else
-                            v[i] = make_float2(S::raw(r[0]), S::raw(r[1]));
+                            v[i] = make_float2(S::raw(a), S::raw(b));
                     }
                 });
                 if (collide_pair<Q, S>(v, p.tau, p.cs)) atomicOr(diverged, 1);
@@ -228,12 +278,12 @@ __global__ void __launch_bounds__(kTileThreads, kTileBlocksPerSm) k_bulk_tiles(c
                 float f[Q];
                 static_for<0, Q>([&](auto I) {
                     constexpr int i = decltype(I)::value;
-                    f[i] = S::dec(sm[i * kBox + b - L::ex(i)], L::w(i));
+                    f[i] = S::dec(*src(st, I, b), L::w(i));
                 });
                 if (collide<Q, S::kExact>(f, p.tau, p.cs)) atomicOr(diverged, 1);
                 static_for<0, Q>([&](auto I) {
                     constexpr int i = decltype(I)::value;
-                    store_pop_i<Q, S, i>(static_cast<T*>(pp.dst[0]), g.n, c + (uint32_t)b, f[i]);
+                    store_pop_i<Q, S, i>(fout, g.n, c + (uint32_t)b, f[i]);
                 });
             }
         }
@@ -280,16 +330,19 @@ static cudaError_t tiles_t(const void* fin, void* fout, const uint32_t* bits, co
 
         auto encode = tensor_map_encoder();
         if (!encode) return cudaErrorNotSupported;
-        // the whole population set as nx columns x (Q * nz * ny) rows of 16-bit elements
-        CUtensorMap map{};
+        // the whole population set as nx columns x (Q * nz * ny) rows of 16-bit
+        // elements, read as 64 x 8 main boxes and 8 x 8 (16-byte) halo boxes
         const cuuint64_t dims[2] = {(cuuint64_t)g.nx, (cuuint64_t)Q * g.nz * g.ny};
         const cuuint64_t strides[1] = {(cuuint64_t)g.nx * S::kBytes};
-        const cuuint32_t box[2] = {(cuuint32_t)St::kCols, (cuuint32_t)kTileRows};
         const cuuint32_t estr[2] = {1, 1};
-        if (encode(&map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, const_cast<void*>(fin), dims, strides, box, estr,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-            return cudaErrorInvalidValue;
+        CUtensorMap maps[2] = {};
+        const cuuint32_t boxes[2][2] = {{(cuuint32_t)St::kCols, (cuuint32_t)kTileRows},
+                                        {(cuuint32_t)St::kHaloCols, (cuuint32_t)kTileRows}};
+        for (int m = 0; m < 2; ++m)
+            if (encode(&maps[m], CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, const_cast<void*>(fin), dims, strides, boxes[m],
+                       estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                return cudaErrorInvalidValue;
 
         PlanePtrs pp{};
         for (int i = 0; i < Q; ++i) {
@@ -314,7 +367,8 @@ static cudaError_t tiles_t(const void* fin, void* fout, const uint32_t* bits, co
         }
         unsigned long long blocks = (unsigned long long)blocks_dev[dev];
         if (blocks > plan.tiles) blocks = plan.tiles;
-        k_bulk_tiles<Q, S><<<(unsigned)blocks, kTileThreads, St::kSmem, s>>>(map, bits, g, p, pp, plan, dv);
+        k_bulk_tiles<Q, S><<<(unsigned)blocks, kTileThreads, St::kSmem, s>>>(
+            maps[0], maps[1], bits, g, p, pp, plan, dv);
         ++*launched;
         return cudaGetLastError();
     }

@@ -14,12 +14,14 @@ pytestmark = pytest.mark.gpu
 
 # (nx, ny, nz), sphere (cx, cy, cz, r), params: several interior chunks per
 # row, a single one (nx = 136), walls cutting interior rows, both flow
-# directions, every slip setting
+# directions, every slip setting; the last sphere's rows end on both sides of
+# the chunk edge x = 128, so one-cell updates read the halo columns
 LATTICES = [
     ((320, 36, 30), (90.0, 18.0, 15.0, 7.0), dict(tau=0.56, inlet_velocity=0.06, smagorinsky_cs=0.1)),
     ((136, 24, 20), (60.0, 12.0, 10.0, 5.0),
      dict(tau=0.6, inlet_velocity=0.05, smagorinsky_cs=0.12, reverse_flow=1, free_slip_y=0)),
     ((200, 18, 26), (70.0, 9.0, 13.0, 4.5), dict(tau=0.58, inlet_velocity=0.05, smagorinsky_cs=0.0, free_slip_z=0)),
+    ((256, 22, 24), (131.5, 11.0, 12.0, 6.5), dict(tau=0.57, inlet_velocity=0.06, smagorinsky_cs=0.1)),
 ]
 
 
