@@ -156,26 +156,33 @@ __device__ __forceinline__ void plane_cell(const typename S::T* __restrict__ fin
 //     outlet cell.
 // Stores the pair's post-collision values (full floats for the exact
 // format, scaled offsets otherwise): one 2-element store per plane for a full
-// pair, element stores for the valid cell of a partial one.
+// pair, element stores for the valid cell of a partial one. The full / partial
+// test is made once for all Q planes: per plane it costs a divergence-safe
+// branch (BSSY / BSYNC) for each of the Q stores.
 template <int Q, class S>
 __device__ __forceinline__ void store_pair(const PlanePtrs& pp, uint32_t c, const float2 (&v)[Q], unsigned pair) {
     using L = Lattice<Q>;
     using T = typename S::T;
-    static_for<0, Q>([&](auto I) {
+    auto enc = [&](auto I) {
         constexpr int i = decltype(I)::value;
-        T* dst = static_cast<T*>(pp.dst[i]);
-        typename S::T2 h;
         if constexpr (S::kExact)
-            h = S::enc2(v[i].x, v[i].y, L::w(i));
+            return S::enc2(v[i].x, v[i].y, L::w(i));
         else
-            h = S::pack2(v[i].x, v[i].y);
-        if (pair == 3u) {
-            *reinterpret_cast<typename S::T2*>(dst + c) = h;
-        } else {
+            return S::pack2(v[i].x, v[i].y);
+    };
+    if (pair == 3u) {
+        static_for<0, Q>([&](auto I) {
+            T* dst = static_cast<T*>(pp.dst[decltype(I)::value]);
+            *reinterpret_cast<typename S::T2*>(dst + c) = enc(I);
+        });
+    } else {
+        static_for<0, Q>([&](auto I) {
+            T* dst = static_cast<T*>(pp.dst[decltype(I)::value]);
+            const typename S::T2 h = enc(I);
             if (pair & 1u) dst[c] = h.x;
             if (pair & 2u) dst[c + 1u] = h.y;
-        }
-    });
+        });
+    }
 }
 
 // Blocks of k_bulk_pairs when its interior warps run in k_bulk_tiles: the
