@@ -18,6 +18,13 @@ per cell on the tensor cores inside the collision); FP16 with plain
 Smagorinsky and the plain FP32 path (bit-identical to the reference) are
 timed beside it.
 
+The learned variants are timed in the developed flow: after ``--spinup``
+untimed steps from the seed (default 2000 of the configuration's 3000-step
+run). The MLP runs only in warps with a cell whose inputs are in its
+training range, and that share grows from about a fifth of the warps in the
+first hundred steps to nearly all of them once the wake has developed. The
+plain variants do the same work in every flow state.
+
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 For N > 1 run under torchrun; every rank steps its own lattice (replicas, no
 data-path collective).
@@ -60,9 +67,10 @@ CONFIGS = {
 }
 
 BYTES_PER_ELEM = {"fp32": 4, "fp16_offset": 2, "bf16_offset": 2, "fp16_learned": 2, "bf16_learned": 2,
-                  "fp32_aa": 4, "fp16_aa": 2, "bf16_aa": 2, "fp16_tma": 2}
+                  "fp32_aa": 4, "fp16_aa": 2, "bf16_aa": 2, "fp16_tma": 2, "fp16_aa_learned": 2,
+                  "bf16_aa_learned": 2}
 # per-cell bytes beyond the populations: the closure's wall-distance byte
-EXTRA_BYTES = {"fp16_learned": 1, "bf16_learned": 1}
+EXTRA_BYTES = {"fp16_learned": 1, "bf16_learned": 1, "fp16_aa_learned": 1, "bf16_aa_learned": 1}
 CLOSURE_WEIGHTS = os.path.join(ROOT, "flowcraft_b200", "data", "closure_c4.json")
 
 
@@ -73,8 +81,11 @@ def parse_args(argv=None):
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="large")
-    ap.add_argument("--variants", default="fp16_learned,fp16_offset,fp32,fp16_aa,fp32_aa",
-                    help="first one is the headline; *_aa: one population set streamed in place")
+    ap.add_argument("--variants", default="fp16_learned,fp16_offset,fp32,fp16_aa,fp32_aa,fp16_aa_learned",
+                    help="first one is the headline; *_aa*: one population set streamed in place; "
+                         "*_learned: the learned closure")
+    ap.add_argument("--spinup", type=int, default=2000,
+                    help="untimed steps from the seed before the warm-up of the learned variants (flow state)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -183,13 +194,25 @@ def storage_of(variant):
     from flowcraft_b200 import Storage
     return {"fp32": Storage.FP32, "fp16_offset": Storage.FP16_OFFSET, "bf16_offset": Storage.BF16_OFFSET,
             "fp16_learned": Storage.FP16_OFFSET, "bf16_learned": Storage.BF16_OFFSET, "fp32_aa": Storage.FP32,
-            "fp16_aa": Storage.FP16_OFFSET, "bf16_aa": Storage.BF16_OFFSET, "fp16_tma": Storage.FP16_OFFSET}[variant]
+            "fp16_aa": Storage.FP16_OFFSET, "bf16_aa": Storage.BF16_OFFSET, "fp16_tma": Storage.FP16_OFFSET,
+            "fp16_aa_learned": Storage.FP16_OFFSET, "bf16_aa_learned": Storage.BF16_OFFSET}[variant]
 
 
 def streaming_of(variant):
-    """The *_aa variants keep one population set streamed in place."""
+    """The *_aa* variants keep one population set streamed in place."""
     from flowcraft_b200 import Streaming
-    return Streaming.AA if variant.endswith("_aa") else Streaming.PINGPONG
+    return Streaming.AA if "_aa" in variant else Streaming.PINGPONG
+
+
+def spinup_of(args, variant) -> int:
+    """Untimed steps before the warm-up: the learned variants' cost depends on
+    the flow state (how many warps run the MLP), the others' does not."""
+    return args.spinup if variant.endswith("_learned") else 0
+
+
+def kernel_of(variant) -> str:
+    name = "k_bulk_pairs" + ("_aa" if "_aa" in variant else "") + ("_learned" if variant.endswith("_learned") else "")
+    return f"{name}<19,{variant}>"
 
 
 def make_solver(cfg, solid, sdf, variant, device_index):
@@ -296,7 +319,7 @@ def run_reference_arm(args, cfg, rank, world):
 def time_variant(args, cfg, solid, sdf, variant, dev_index, dist_on, sample_clocks):
     s = make_solver(cfg, solid, sdf, variant, dev_index)
     info = s.BoundaryInfo()
-    s.Step(None, args.warmup)
+    s.Step(None, spinup_of(args, variant) + args.warmup)
     s.Sync()
     barrier_sync(dist_on)
     sampler = ClockSampler(dev_index) if sample_clocks else None
@@ -322,6 +345,7 @@ def time_variant(args, cfg, solid, sdf, variant, dev_index, dist_on, sample_cloc
         "bouzidi_links": info["bouzidi_links"], "bulk_bytes_per_launch": bulk_bytes,
         "bulk_gbs": bulk_bytes / bulk_avg_s / 1e9 if bulk_avg_s > 0 else None,
         "launches": launches, "clocks": clocks, "bytes_per_cell": per_cell, "closure_coverage": coverage,
+        "spinup_steps": spinup_of(args, variant),
         "stats_after": {"avg_density": stats.avgDensity, "avg_speed": stats.avgSpeed, "has_nan": stats.hasNaN,
                         "force_x": stats.forceX, "force_z": stats.forceZ},
     }
@@ -331,11 +355,13 @@ def run_e2e(args, cfg, solid, sdf, variant, dev_index):
     """The same metric end to end through the public API with host buffers:
     Init from pinned host geometry (H2D), Reset, then per step Step(1) plus
     ProbeSliceHealth of one z-layer (D2H), then ReadbackStats and the full
-    4-float field into host memory (D2H). Wall clock around the host calls."""
+    4-float field into host memory (D2H). Wall clock around the host calls.
+    For the learned variants the spin-up steps are part of the job and of the
+    timed region, so the number is the whole run's rate from the seed."""
     import numpy as np
     import torch
 
-    from flowcraft_b200 import LatticeModel, LbmSolver, Params, Storage, VoxelGrid
+    from flowcraft_b200 import LatticeModel, LbmSolver, Params, VoxelGrid
     h_solid = solid.cpu().pin_memory()
     h_sdf = sdf.cpu().pin_memory()
     n = cfg["nx"] * cfg["ny"] * cfg["nz"]
@@ -343,18 +369,19 @@ def run_e2e(args, cfg, solid, sdf, variant, dev_index):
     out[::1024] = 0  # fault the pages in before timing
     out.fill(0)
     st = storage_of(variant)
+    steps = spinup_of(args, variant) + args.steps
     grid = VoxelGrid(cfg["nx"], cfg["ny"], cfg["nz"], solid=h_solid.numpy(), signedDistance=h_sdf.numpy())
     torch.cuda.synchronize()
     s = LbmSolver()
     t0 = time.perf_counter()
-    if not s.Init(dev_index, grid, LatticeModel.D3Q19, st):
+    if not s.Init(dev_index, grid, LatticeModel.D3Q19, st, streaming_of(variant)):
         raise RuntimeError(s.LastError())
     s.Reset(Params(tau=tau_for(cfg), inletVelocity=cfg["u"], smagorinskyCs=cfg["cs"]), True)
     if variant.endswith("_learned"):
         from flowcraft_b200.closure import ClosureWeights
         s.SetClosure(ClosureWeights.load(CLOSURE_WEIGHTS))
     diverged = False
-    for k in range(args.steps):
+    for k in range(steps):
         s.Step(None, 1)
         diverged |= s.ProbeSliceHealth(k % cfg["nz"])
     stats = s.ReadbackStats()
@@ -363,12 +390,13 @@ def run_e2e(args, cfg, solid, sdf, variant, dev_index):
     s.close()
     layer = cfg["nx"] * cfg["ny"] * 16
     h2d = n * (1 + 4)
-    d2h = layer * args.steps + n * 16 + 96
-    return {"value": n * args.steps / el / 1e9, "unit": "GLUPS", "seconds": el,
-            "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
+    d2h = layer * steps + n * 16 + 96
+    return {"value": n * steps / el / 1e9, "unit": "GLUPS", "seconds": el, "steps": steps,
+            "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps,
             "diverged": diverged, "avg_density": stats.avgDensity,
             "timed": "Init(host VoxelGrid) + Reset + SetClosure (learned variants) + steps x (Step(1) + "
-                     "ProbeSliceHealth) + ReadbackStats + ReadbackFieldRange(all z)"}
+                     "ProbeSliceHealth) + ReadbackStats + ReadbackFieldRange(all z); steps = spin-up + timed "
+                     "steps for the learned variants"}
 
 
 def run_batch(args, cfg, rank, world, local_rank):
@@ -456,8 +484,7 @@ def run_ours(args, cfg, rank, world, local_rank):
         "bound": "hbm", "achieved": head["bulk_gbs"], "peak": peak, "unit": "GB/s",
         "frac": head["bulk_gbs"] / peak if head["bulk_gbs"] else None,
         "traffic": trf * head["bulk_cells"] if trf else None,
-        "kernel": (f"k_bulk_pairs_learned<19,{head['variant']}>" if head["variant"].endswith("_learned")
-                   else f"k_bulk_pairs<19,{head['variant']}>") + " (all bulk-mask cells)",
+        "kernel": kernel_of(head["variant"]) + " (all bulk-mask cells)",
         "algorithmic_bytes_per_launch": head["bulk_bytes_per_launch"],
         "peak_source": f"{peak_src} ({'MEASURED_PEAKS.json hbm_gbs' if peak_src == 'measured' else 'fallback'})",
     }
@@ -482,7 +509,7 @@ def run_ours(args, cfg, rank, world, local_rank):
             "bulk_ms_per_launch": r["bulk_ms_per_launch"], "boundary_ms_per_launch": r["boundary_ms_per_launch"],
             "bulk_gbs": r["bulk_gbs"], "roofline_frac": r["bulk_gbs"] / peak if r["bulk_gbs"] else None,
             "bytes_per_cell_update": r["bytes_per_cell"], "clocks": r["clocks"], "stats_after": r["stats_after"],
-            "closure_coverage": r["closure_coverage"],
+            "closure_coverage": r["closure_coverage"], "spinup_steps": r["spinup_steps"],
         }
     line = {
         "metric": METRIC, "value": value, "unit": "GLUPS", "n_gpus": world, "steps": args.steps,
@@ -494,7 +521,9 @@ def run_ours(args, cfg, rank, world, local_rank):
                    "closure": ("learned MLP 5-32-32-1 (BF16 tensor-core MMA, FP32 accumulate) per cell, Smagorinsky "
                                "Cs=0.1 outside its training range; weights flowcraft_b200/data/closure_c4.json"
                                if head["variant"].endswith("_learned") else "Smagorinsky"),
-                   "streaming": "pull, ping-pong",
+                   "streaming": "AA pattern, one set in place" if "_aa" in head["variant"] else "pull, ping-pong",
+                   "flow_state": (f"timed after {head['spinup_steps']} + {args.warmup} steps from the mid-speed seed"
+                                  if head["spinup_steps"] else f"timed after {args.warmup} steps from the seed"),
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "no flush: the population set (10.2 GB fp16 / 20.4 GB fp32 per copy) exceeds the 126 MB L2",
                    "boundary_cells": head["boundary_cells"], "bouzidi_links": head["bouzidi_links"]},

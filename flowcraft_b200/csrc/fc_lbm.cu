@@ -388,6 +388,9 @@ int guard_snapshot(fc_lbm* h, cudaStream_t s, int set) {
 // The two step kernels, with or without the learned closure, ping-pong or in place.
 cudaError_t launch_bulk(fc_lbm* h, const fc::StepParams& p, const void* fin, void* fout, int z0, int zc,
                         cudaStream_t s, int* nl) {
+    if (in_place(h) && h->closure_on)
+        return fc::launch_bulk_aa_learned(h->q, h->storage, h->pop[0], h->d_bulk_bits, h->g, p, z0, zc,
+                                          h->d_diverged, s, nl, h->cur, aa_side(h), h->closure);
     if (in_place(h))
         return fc::launch_bulk_aa(h->q, h->storage, h->pop[0], h->d_bulk_bits, h->g, p, z0, zc, h->d_diverged, s, nl,
                                   h->cur, aa_side(h));
@@ -401,6 +404,9 @@ cudaError_t launch_bulk(fc_lbm* h, const fc::StepParams& p, const void* fin, voi
 cudaError_t launch_boundary(fc_lbm* h, const fc::StepParams& p, const void* fin, void* fout, uint32_t b, uint32_t e,
                             cudaStream_t s) {
     const fc::BoundaryList bl = boundary_list(h);
+    if (in_place(h) && h->closure_on)
+        return fc::launch_boundary_aa_learned(h->q, h->storage, h->pop[0], bl, b, e, h->g, p, h->d_diverged, s,
+                                              h->cur, aa_side(h), h->closure);
     if (in_place(h))
         return fc::launch_boundary_aa(h->q, h->storage, h->pop[0], bl, b, e, h->g, p, h->d_diverged, s, h->cur,
                                       aa_side(h));
@@ -793,7 +799,6 @@ int fc_lbm_set_closure(fc_lbm* h, const fc_closure* c) {
     if (h->storage == FC_STORAGE_FP32)
         return fail(h, FC_LBM_ERR_UNSUPPORTED, "the learned closure runs on the FP16/BF16 offset storage formats");
     if (h->g.nx % 2 != 0) return fail(h, FC_LBM_ERR_UNSUPPORTED, "the learned closure needs an even nx");
-    if (in_place(h)) return fail(h, FC_LBM_ERR_UNSUPPORTED, "the learned closure runs with ping-pong streaming");
     if (!c->w1 || !c->b1 || !c->w2 || !c->b2 || !c->w3)
         return fail(h, FC_LBM_ERR_INVALID_ARG, "closure weights missing");
     bool ok = std::isfinite(c->b3) && std::isfinite(c->out_scale) && c->out_scale > 0.0f &&
@@ -870,8 +875,8 @@ int fc_lbm_closure_probe(fc_lbm* h, float* out, uint8_t* in_range, size_t cells)
     FC_TRY(h, cudaMalloc(&d_out, h->g.n * 5 * sizeof(float)), "alloc probe");
     cudaError_t e = cudaMalloc(&d_rng, h->g.n);
     if (e == cudaSuccess)
-        e = fc::launch_closure_probe(h->q, h->storage, h->pop[h->cur], h->g, h->closure, d_out, d_rng, nullptr,
-                                     h->stream);
+        e = fc::launch_closure_probe(h->q, h->storage, h->pop[h->cur], h->d_solid, h->g, h->closure, d_out, d_rng,
+                                     nullptr, layout_of(h), h->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(out, d_out, h->g.n * 5 * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(in_range, d_rng, h->g.n, cudaMemcpyDeviceToHost, h->stream);
@@ -889,8 +894,8 @@ int fc_lbm_closure_coverage(fc_lbm* h, uint64_t* cells_in_range, uint64_t* warps
     DeviceGuard dg(h->device);
     unsigned long long* d = reinterpret_cast<unsigned long long*>(h->d_stats_result);  // 2 slots, reused
     FC_TRY(h, cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), h->stream), "clear counts");
-    FC_TRY(h, fc::launch_closure_probe(h->q, h->storage, h->pop[h->cur], h->g, h->closure, nullptr, nullptr, d,
-                                       h->stream),
+    FC_TRY(h, fc::launch_closure_probe(h->q, h->storage, h->pop[h->cur], h->d_solid, h->g, h->closure, nullptr,
+                                       nullptr, d, layout_of(h), h->stream),
            "closure coverage");
     h->launches++;
     FC_TRY(h, cudaMemcpyAsync(h->h_stage, d, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream),

@@ -118,8 +118,9 @@ int closure_samples(int q, int storage, const void* f, const uint8_t* solid, con
 cudaError_t launch_bulk_pull_learned(int q, int storage, const void* fin, void* fout, const uint32_t* bulk_bits,
                                      const Geom& g, const StepParams& p, int z0, int zc, int* diverged,
                                      cudaStream_t s, int* launched, const ClosureDev& cl);
-cudaError_t launch_closure_probe(int q, int storage, const void* f, const Geom& g, const ClosureDev& cl, float* out,
-                                 uint8_t* in_range, unsigned long long* counts, cudaStream_t s);
+cudaError_t launch_closure_probe(int q, int storage, const void* f, const uint8_t* solid, const Geom& g,
+                                 const ClosureDev& cl, float* out, uint8_t* in_range, unsigned long long* counts,
+                                 int layout, cudaStream_t s);
 
 // One lattice of a batch (fc_lbm_batch): everything the persistent bulk
 // kernel needs, in device memory. pp[k] are the plane pointers of a step that
@@ -170,6 +171,13 @@ cudaError_t launch_bulk_aa(int q, int storage, void* f, const uint32_t* bulk_bit
 cudaError_t launch_boundary_aa(int q, int storage, void* f, const BoundaryList& bl, uint32_t begin, uint32_t end,
                                const Geom& g, const StepParams& p, int* diverged, cudaStream_t s, int odd,
                                const AaSide& sd);
+// The same with the learned closure (16-bit offset formats).
+cudaError_t launch_bulk_aa_learned(int q, int storage, void* f, const uint32_t* bulk_bits, const Geom& g,
+                                   const StepParams& p, int z0, int zc, int* diverged, cudaStream_t s, int* launched,
+                                   int odd, const AaSide& sd, const ClosureDev& cl);
+cudaError_t launch_boundary_aa_learned(int q, int storage, void* f, const BoundaryList& bl, uint32_t begin,
+                                       uint32_t end, const Geom& g, const StepParams& p, int* diverged,
+                                       cudaStream_t s, int odd, const AaSide& sd, const ClosureDev& cl);
 // Fills the side buffers from the state a step of parity `par` reads (after a
 // seed or a population load); `count` = boundary-list length.
 cudaError_t launch_aa_prime(int q, int storage, const void* f, const BoundaryList& bl, uint32_t count, const Geom& g,

@@ -20,6 +20,7 @@
 //
 // Both kernels read one population set and write the other (ping-pong), so
 // they are independent and touch disjoint cells.
+#include "aa.cuh"
 #include "closure.cuh"
 #include "collide.cuh"
 #include "collide2.cuh"
@@ -447,40 +448,54 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned(const 
 }
 
 // The closure's inputs and nu_t for every cell of the current population set
-// as stored (no streaming): the same device code as the fused kernels, for
-// checking the inference against a CPU evaluation. Two cells per lane.
+// as stored (no streaming; `layout` a PopLayout of aa.cuh): the same device
+// code as the fused kernels, for checking the inference against a CPU
+// evaluation. Two cells per lane. Solid cells count as holding f = w, what
+// a ping-pong set keeps there (in place their slots carry the neighbours'
+// bounced populations).
 // out[5*c .. 5*c+4] = inputs 0-3 and nu_t; in_range[c] = 1 when the learned
 // value is used. With out == nullptr it only counts, into counts[0] the
 // cells in range and into counts[1] the 64-cell warps with any cell in range
 // (the warps that run the MLP in a step).
 template <int Q, class S>
-__global__ void __launch_bounds__(128) k_closure_probe(const typename S::T* __restrict__ f, Geom g, ClosureDev cl,
+__global__ void __launch_bounds__(128) k_closure_probe(const typename S::T* __restrict__ f,
+                                                       const uint8_t* __restrict__ solid, Geom g, ClosureDev cl,
                                                        float* __restrict__ out, uint8_t* __restrict__ in_range,
-                                                       unsigned long long* __restrict__ counts) {
+                                                       unsigned long long* __restrict__ counts, int layout) {
     static_assert(!S::kExact, "the learned closure runs on the 16-bit offset formats");
     __shared__ uint32_t s_in[4][32 * 8];
     __shared__ float2 s_out[4][32];
     const size_t c = 2 * ((size_t)blockIdx.x * blockDim.x + threadIdx.x);
     const bool ha = c < g.n, hb = c + 1 < g.n;
+    const bool la = ha && !solid[c], lb = hb && !solid[c + 1];  // read the stored values
+    auto coords = [&](size_t cc, int& x, int& y, int& z) {
+        z = (int)(cc / g.nxy);
+        const size_t rem = cc - (size_t)z * g.nxy;
+        y = (int)(rem / (size_t)g.nx);
+        x = (int)(rem - (size_t)y * g.nx);
+    };
+    int xa = 0, ya = 0, za = 0, xb = 0, yb = 0, zb = 0;
+    if (ha) coords(c, xa, ya, za);
+    if (hb) coords(c + 1, xb, yb, zb);
     float2 v[Q];
     static_for<0, Q>([&](auto I) {
         constexpr int i = decltype(I)::value;
-        v[i] = make_float2(ha ? S::raw(S::ld(f + (size_t)i * g.n + c)) : 0.0f,
-                           hb ? S::raw(S::ld(f + (size_t)i * g.n + c + 1)) : 0.0f);
+        v[i] = make_float2(la ? S::raw(S::ld(f + pop_slot<Q, i>(c, xa, ya, za, g, layout))) : 0.0f,
+                           lb ? S::raw(S::ld(f + pop_slot<Q, i>(c + 1, xb, yb, zb, g, layout))) : 0.0f);
     });
     Mom2 mo;
     moments2<Q>(v, mo);
-    float xa[4], xb[4];
-    closure_invariants(mo.pxx.x, mo.pyy.x, mo.pzz.x, mo.pxy.x, mo.pxz.x, mo.pyz.x, mo.pp.x, mo.inv.x, xa[0], xa[1],
-                       xa[2]);
-    closure_invariants(mo.pxx.y, mo.pyy.y, mo.pzz.y, mo.pxy.y, mo.pxz.y, mo.pyz.y, mo.pp.y, mo.inv.y, xb[0], xb[1],
-                       xb[2]);
-    xa[3] = ha ? (float)cl.wall[c] * 0.0625f : 0.0f;
-    xb[3] = hb ? (float)cl.wall[c + 1] * 0.0625f : 0.0f;
+    float ia[4], ib[4];
+    closure_invariants(mo.pxx.x, mo.pyy.x, mo.pzz.x, mo.pxy.x, mo.pxz.x, mo.pyz.x, mo.pp.x, mo.inv.x, ia[0], ia[1],
+                       ia[2]);
+    closure_invariants(mo.pxx.y, mo.pyy.y, mo.pzz.y, mo.pxy.y, mo.pxz.y, mo.pyz.y, mo.pp.y, mo.inv.y, ib[0], ib[1],
+                       ib[2]);
+    ia[3] = ha ? (float)cl.wall[c] * 0.0625f : 0.0f;
+    ib[3] = hb ? (float)cl.wall[c + 1] * 0.0625f : 0.0f;
     const int warp = threadIdx.x >> 5;
     if (!out) {
-        const bool ra = ha && closure_in_range(cl, xa[0], xa[1], xa[2]);
-        const bool rb = hb && closure_in_range(cl, xb[0], xb[1], xb[2]);
+        const bool ra = ha && closure_in_range(cl, ia[0], ia[1], ia[2]);
+        const bool rb = hb && closure_in_range(cl, ib[0], ib[1], ib[2]);
         const unsigned cells = __popc(__ballot_sync(0xffffffffu, ra)) + __popc(__ballot_sync(0xffffffffu, rb));
         if ((threadIdx.x & 31) == 0 && cells) {
             atomicAdd(counts, (unsigned long long)cells);
@@ -489,19 +504,19 @@ __global__ void __launch_bounds__(128) k_closure_probe(const typename S::T* __re
         return;
     }
     uint32_t* in = &s_in[warp][(threadIdx.x & 31) * 8];
-    closure_pack_inputs(cl, xa[0], xa[1], xa[2], xa[3], in);
-    closure_pack_inputs(cl, xb[0], xb[1], xb[2], xb[3], in + 4);
+    closure_pack_inputs(cl, ia[0], ia[1], ia[2], ia[3], in);
+    closure_pack_inputs(cl, ib[0], ib[1], ib[2], ib[3], in + 4);
     __syncwarp();
     const float2 nu = closure_warp_mlp(cl.frag, s_in[warp], s_out[warp]);
     if (ha) {
-        for (int k = 0; k < 4; ++k) out[5 * c + k] = xa[k];
+        for (int k = 0; k < 4; ++k) out[5 * c + k] = ia[k];
         out[5 * c + 4] = nu.x;
-        in_range[c] = closure_in_range(cl, xa[0], xa[1], xa[2]) ? 1 : 0;
+        in_range[c] = closure_in_range(cl, ia[0], ia[1], ia[2]) ? 1 : 0;
     }
     if (hb) {
-        for (int k = 0; k < 4; ++k) out[5 * (c + 1) + k] = xb[k];
+        for (int k = 0; k < 4; ++k) out[5 * (c + 1) + k] = ib[k];
         out[5 * (c + 1) + 4] = nu.y;
-        in_range[c + 1] = closure_in_range(cl, xb[0], xb[1], xb[2]) ? 1 : 0;
+        in_range[c + 1] = closure_in_range(cl, ib[0], ib[1], ib[2]) ? 1 : 0;
     }
 }
 
@@ -975,14 +990,15 @@ static cudaError_t boundary_learned_t(const void* fin, void* fout, const Boundar
 }
 
 template <int Q, class S>
-static cudaError_t closure_probe_t(const void* f, const Geom& g, const ClosureDev& cl, float* out, uint8_t* in_range,
-                                   unsigned long long* counts, cudaStream_t s) {
+static cudaError_t closure_probe_t(const void* f, const uint8_t* solid, const Geom& g, const ClosureDev& cl,
+                                   float* out, uint8_t* in_range, unsigned long long* counts, int layout,
+                                   cudaStream_t s) {
     if constexpr (S::kExact) {
         return cudaErrorNotSupported;
     } else {
         const size_t pairs = (g.n + 1) / 2;
-        k_closure_probe<Q, S><<<(unsigned)((pairs + 127) / 128), 128, 0, s>>>((const typename S::T*)f, g, cl, out,
-                                                                              in_range, counts);
+        k_closure_probe<Q, S><<<(unsigned)((pairs + 127) / 128), 128, 0, s>>>((const typename S::T*)f, solid, g, cl,
+                                                                              out, in_range, counts, layout);
         return cudaGetLastError();
     }
 }
@@ -1076,9 +1092,10 @@ int bulk_batch_resident(int q, int storage, int rows) {
     return batch_resident_dispatch(q, storage, rows, &nb) == cudaSuccess ? nb : 0;
 }
 
-cudaError_t launch_closure_probe(int q, int storage, const void* f, const Geom& g, const ClosureDev& cl, float* out,
-                                 uint8_t* in_range, unsigned long long* counts, cudaStream_t s) {
-    FC_DISPATCH(q, storage, closure_probe_t, f, g, cl, out, in_range, counts, s);
+cudaError_t launch_closure_probe(int q, int storage, const void* f, const uint8_t* solid, const Geom& g,
+                                 const ClosureDev& cl, float* out, uint8_t* in_range, unsigned long long* counts,
+                                 int layout, cudaStream_t s) {
+    FC_DISPATCH(q, storage, closure_probe_t, f, solid, g, cl, out, in_range, counts, layout, s);
 }
 
 }  // namespace fc

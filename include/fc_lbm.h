@@ -60,9 +60,9 @@ extern "C" {
 
 /* Streaming scheme. PINGPONG keeps two population copies (pull scheme, the
  * reference's layout); AA keeps one copy updated in place, half the device
- * memory, with results bit-identical to PINGPONG. AA needs an even nx >= 4
- * and does not combine with the learned closure, batches, closure samples
- * or layer copies (FC_LBM_ERR_UNSUPPORTED). */
+ * memory, with results bit-identical to PINGPONG (also with the learned
+ * closure). AA needs an even nx >= 4 and does not combine with batches,
+ * closure samples or layer copies (FC_LBM_ERR_UNSUPPORTED). */
 #define FC_STREAMING_PINGPONG 0
 #define FC_STREAMING_AA 1
 
@@ -272,9 +272,9 @@ typedef struct fc_closure {
 } fc_closure;
 
 /* Installs the closure (copied; NULL returns to Smagorinsky) for every later
- * step. Needs FP16/BF16 offset storage and an even nx
- * (FC_LBM_ERR_UNSUPPORTED otherwise). The first call computes the wall
- * distance field (one byte per cell). Blocking. */
+ * step, under either streaming scheme. Needs FP16/BF16 offset storage and an
+ * even nx (FC_LBM_ERR_UNSUPPORTED otherwise). The first call computes the
+ * wall distance field (one byte per cell). Blocking. */
 FC_LBM_API int fc_lbm_set_closure(fc_lbm* h, const fc_closure* c);
 /* The closure evaluated on the current populations as stored, by the same
  * device code as the step: out[5*c .. 5*c+4] = inputs 0-3 and nu_t,

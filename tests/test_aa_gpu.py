@@ -6,7 +6,8 @@ golden cases, and every format must give bit-identical fields, statistics,
 forces and populations to ping-pong on lattices that route cells through
 every branch: Bouzidi near and far links, plain bounce-back, free-slip and
 no-slip faces, inlet and outlet in both flow directions (flipped live), solid
-outlet neighbours, and a warm start from a field.
+outlet neighbours, and a warm start from a field; with the learned closure
+too.
 """
 import numpy as np
 import pytest
@@ -129,6 +130,67 @@ def test_aa_bit_identical_to_pingpong(gpu, name, storage):
     assert info["boundary_cells"] > 0 and info["bulk_cells"] > 0
 
 
+def _closure_for(sim, seed):
+    """Random weights normalized to the lattice's own inputs, with a training
+    range that leaves the tails out, so both the MLP and the Smagorinsky
+    fallback run."""
+    from flowcraft_b200.closure import ClosureWeights
+    cw = ClosureWeights.random(seed, 2e-3)
+    sim.s.SetClosure(cw)
+    x, _, _ = sim.s.ClosureProbe()
+    fluid = ~sim.solid
+    cw.mean[:4] = x[fluid].mean(axis=0)
+    cw.std[:4] = np.maximum(x[fluid].std(axis=0), 1e-3)
+    cw.mean[4], cw.std[4], cw.filter_width = 1.0, 1.0, 1.0
+    cw.lo = np.percentile(x[fluid][:, :3], 3.0, axis=0).astype(np.float32)
+    cw.hi = np.percentile(x[fluid][:, :3], 97.0, axis=0).astype(np.float32)
+    return cw
+
+
+@pytest.mark.parametrize("storage", ["FP16_OFFSET", "BF16_OFFSET"])
+@pytest.mark.parametrize("name", ["noslip_reverse", "ground_q15", "outlet_block", "wide_q15", "wide_nosdf"])
+def test_aa_learned_closure_bit_identical_to_pingpong(gpu, name, storage):
+    """The learned closure in place: the same MLP inputs, fallbacks and stored
+    values as the ping-pong learned step, so fields, populations and the
+    coverage probe agree bit for bit, with a live flow reversal."""
+    case = BRANCHES[name]
+    pp, aa = Sim(case, storage, "PINGPONG"), Sim(case, storage, "AA")
+    pp.step(3)
+    aa.step(3)
+    cw = _closure_for(pp, 11)
+    for sim in (pp, aa):
+        sim.s.SetClosure(cw)
+    cov = pp.s.ClosureCoverage()
+    assert cov == aa.s.ClosureCoverage()
+    fluid = int((~pp.solid).sum())
+    assert 0 < cov["cells_in_range"] < fluid, cov  # both the MLP and the fallback run
+    for sim in (pp, aa):
+        sim.step(7)
+    _compare(pp, aa, f"{name} learned after 10 steps")
+    xa, na, ra = pp.s.ClosureProbe()
+    xb, nb, rb = aa.s.ClosureProbe()
+    assert _same(xa, xb) and _same(na, nb) and np.array_equal(ra, rb)
+    for sim in (pp, aa):
+        sim.set_params(_flip(case))
+        sim.step(8)
+    _compare(pp, aa, f"{name} learned after 18 steps")
+
+
+def test_aa_learned_step_range_chunks(gpu):
+    """StepRange chunks in place with the closure equal whole steps."""
+    case = BRANCHES["wide_q15"]
+    full, chunks = Sim(case, "FP16_OFFSET"), Sim(case, "FP16_OFFSET")
+    cw = _closure_for(full, 5)
+    for sim in (full, chunks):
+        sim.s.SetClosure(cw)
+    for _ in range(5):
+        full.step(1)
+        for z0 in range(0, 40, 13):
+            chunks.s.StepRange(None, z0, 13)
+        chunks.s.AdvanceSubstep()
+    assert _same(full.s.SavePopulations(), chunks.s.SavePopulations())
+
+
 def test_aa_step_range_chunks_and_warm_start(gpu):
     case = BRANCHES["wide_q15"]
     full, chunks = Sim(case), Sim(case)
@@ -166,18 +228,12 @@ def test_aa_population_load_at_either_parity(gpu, odd):
 
 def test_aa_unsupported_combinations(gpu):
     from flowcraft_b200.batch import LbmBatch
-    from flowcraft_b200.closure import ClosureWeights
     from flowcraft_b200.lbm import LbmSolver, Storage, Streaming, VoxelGrid, LatticeModel
     s = LbmSolver()
     g = VoxelGrid(9, 4, 4, solid=np.zeros(144, np.uint8))
     assert s.Init(0, g, LatticeModel.D3Q19, Storage.FP32, Streaming.AA) is False
     assert "even nx" in s.LastError()
     aa = Sim(BRANCHES["ywall"], "FP16_OFFSET", "AA")
-    import os
-    w = ClosureWeights.load(os.path.join(os.path.dirname(__file__), "..", "flowcraft_b200", "data",
-                                         "closure_c4.json"))
-    with pytest.raises(RuntimeError):
-        aa.s.SetClosure(w)
     with pytest.raises(RuntimeError):
         aa.s.LayerCopy(0, 1, True)
     with pytest.raises(RuntimeError):
