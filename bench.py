@@ -161,16 +161,20 @@ def measured_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def ncu_traffic_per_cell(variant: str):
-    """DRAM bytes per bulk cell update from the committed ncu summary of the
-    bulk kernels (a line 'traffic_bytes_per_cell <variant> = X'), or None."""
-    path = os.path.join(ROOT, "profiles", "bulk_pairs_ncu_c2.md")
-    try:
-        text = open(path).read()
-    except OSError:
-        return None
-    m = re.search(rf"traffic_bytes_per_cell\s+{variant}\s*=\s*([0-9.]+)", text)
-    return float(m.group(1)) if m else None
+def ncu_traffic_per_cell(variant: str, developed: bool = False):
+    """DRAM bytes per bulk cell update from the committed ncu summaries of
+    the bulk kernels (a line 'traffic_bytes_per_cell <variant> = X'; the
+    learned kernel in the developed flow as <variant>_developed), or None."""
+    key = variant + ("_developed" if developed else "")
+    for name in ("bulk_pairs_ncu_c2.md", "bulk_pairs_learned_developed_c2.md"):
+        try:
+            text = open(os.path.join(ROOT, "profiles", name)).read()
+        except OSError:
+            continue
+        m = re.search(rf"traffic_bytes_per_cell\s+{key}\s*=\s*([0-9.]+)", text)
+        if m:
+            return float(m.group(1))
+    return None
 
 
 def build_geometry(cfg, device, z_lo=0, z_hi=None):
@@ -479,7 +483,7 @@ def run_ours(args, cfg, rank, world, local_rank):
     value = world * cells * args.steps / total_s / 1e9
 
     peak, peak_src = measured_peak()
-    trf = ncu_traffic_per_cell(head["variant"])
+    trf = ncu_traffic_per_cell(head["variant"], developed=head["spinup_steps"] > 0)
     roofline = {
         "bound": "hbm", "achieved": head["bulk_gbs"], "peak": peak, "unit": "GB/s",
         "frac": head["bulk_gbs"] / peak if head["bulk_gbs"] else None,
