@@ -68,9 +68,9 @@ CONFIGS = {
 
 BYTES_PER_ELEM = {"fp32": 4, "fp16_offset": 2, "bf16_offset": 2, "fp16_learned": 2, "bf16_learned": 2,
                   "fp32_aa": 4, "fp16_aa": 2, "bf16_aa": 2, "fp16_tma": 2, "fp16_aa_learned": 2,
-                  "bf16_aa_learned": 2}
+                  "bf16_aa_learned": 2, "fp16_tc_learned": 2}
 # per-cell bytes beyond the populations: the closure's wall-distance byte
-EXTRA_BYTES = {"fp16_learned": 1, "bf16_learned": 1, "fp16_aa_learned": 1, "bf16_aa_learned": 1}
+EXTRA_BYTES = {"fp16_learned": 1, "bf16_learned": 1, "fp16_aa_learned": 1, "bf16_aa_learned": 1, "fp16_tc_learned": 1}
 CLOSURE_WEIGHTS = os.path.join(ROOT, "flowcraft_b200", "data", "closure_c4.json")
 
 
@@ -83,7 +83,8 @@ def parse_args(argv=None):
     ap.add_argument("--config", choices=sorted(CONFIGS), default="large")
     ap.add_argument("--variants", default="fp16_learned,fp16_offset,fp32,fp16_aa,fp32_aa,fp16_aa_learned",
                     help="first one is the headline; *_aa*: one population set streamed in place; "
-                         "*_learned: the learned closure")
+                         "*_learned: the learned closure; *_tc_*: its MLP on the tcgen05 tensor cores per block; "
+                         "*_tma: interior rows staged by TMA")
     ap.add_argument("--spinup", type=int, default=2000,
                     help="untimed steps from the seed before the warm-up of the learned variants (flow state)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -199,7 +200,8 @@ def storage_of(variant):
     return {"fp32": Storage.FP32, "fp16_offset": Storage.FP16_OFFSET, "bf16_offset": Storage.BF16_OFFSET,
             "fp16_learned": Storage.FP16_OFFSET, "bf16_learned": Storage.BF16_OFFSET, "fp32_aa": Storage.FP32,
             "fp16_aa": Storage.FP16_OFFSET, "bf16_aa": Storage.BF16_OFFSET, "fp16_tma": Storage.FP16_OFFSET,
-            "fp16_aa_learned": Storage.FP16_OFFSET, "bf16_aa_learned": Storage.BF16_OFFSET}[variant]
+            "fp16_aa_learned": Storage.FP16_OFFSET, "bf16_aa_learned": Storage.BF16_OFFSET,
+            "fp16_tc_learned": Storage.FP16_OFFSET}[variant]
 
 
 def streaming_of(variant):
@@ -215,7 +217,8 @@ def spinup_of(args, variant) -> int:
 
 
 def kernel_of(variant) -> str:
-    name = "k_bulk_pairs" + ("_aa" if "_aa" in variant else "") + ("_learned" if variant.endswith("_learned") else "")
+    name = ("k_bulk_pairs" + ("_aa" if "_aa" in variant else "") + ("_learned" if variant.endswith("_learned") else "")
+            + ("_tc" if "_tc_" in variant else ""))
     return f"{name}<19,{variant}>"
 
 
@@ -223,8 +226,10 @@ def make_solver(cfg, solid, sdf, variant, device_index):
     from flowcraft_b200 import LatticeModel, LbmSolver, Params, VoxelGrid
     s = LbmSolver()
     grid = VoxelGrid(cfg["nx"], cfg["ny"], cfg["nz"], solid=solid, signedDistance=sdf)
-    from flowcraft_b200.lbm import OPTION_TMA_STAGING
+    from flowcraft_b200.lbm import OPTION_TC_CLOSURE, OPTION_TMA_STAGING
     flags = OPTION_TMA_STAGING if variant.endswith("_tma") else 0  # interior rows staged by TMA tensor copies
+    if "_tc_" in variant:
+        flags |= OPTION_TC_CLOSURE  # the closure's MLP on the tcgen05 tensor cores, per block
     if not s.Init(device_index, grid, LatticeModel.D3Q19, storage_of(variant), streaming_of(variant), flags):
         raise RuntimeError(s.LastError())
     s.Reset(Params(tau=tau_for(cfg), inletVelocity=cfg["u"], smagorinskyCs=cfg["cs"]), True)

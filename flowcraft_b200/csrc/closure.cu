@@ -73,6 +73,31 @@ void pack_closure(const float* w1, const float* b1, const float* w2, const float
     }
 }
 
+// The tensor-core MLP's operands B (N x K, K-major): element (n, k) of a
+// block sits at (n / 8) * SBO + (k / 8) * 128 + (n % 8) * 16 + (k % 8) * 2
+// bytes, SBO = K * 16 bytes (one 8-row group of all K core matrices).
+//   W1  bytes    0-1023: n = hidden unit (32), k = input 0-4, 5 the constant 1 (b1), rest 0 (K = 16)
+//   W2  bytes 1024-3071: n = hidden unit of layer 2 (32), k = layer-1 unit (K = 32)
+//   B2  bytes 3072-4095: n = hidden unit of layer 2, k = 0 carries b2, rest 0 (K = 16)
+//   W3  bytes 4096-5119: n = 0 carries w3 * out_scale, rows 1-15 zero (N = 16, K = 32)
+void pack_closure_tc(const float* w1, const float* b1, const float* w2, const float* b2, const float* w3,
+                     float out_scale, uint8_t* out) {
+    constexpr int H = kClosureHidden;
+    std::memset(out, 0, kTcWeightBytes);
+    auto put = [&](int base, int kdim, int n, int k, float v) {
+        const uint16_t b = to_bf16(v);
+        const int off = base + (n / 8) * (kdim * 16) + (k / 8) * 128 + (n % 8) * 16 + (k % 8) * 2;
+        std::memcpy(out + off, &b, 2);
+    };
+    for (int n = 0; n < H; ++n) {
+        for (int k = 0; k < kClosureIn; ++k) put(0, 16, n, k, w1[k * H + n]);
+        put(0, 16, n, kClosureIn, b1[n]);
+        for (int k = 0; k < H; ++k) put(1024, 32, n, k, w2[k * H + n]);
+        put(3072, 16, n, 0, b2[n]);
+    }
+    for (int k = 0; k < H; ++k) put(4096, 32, 0, k, w3[k] * out_scale);
+}
+
 namespace {
 
 __global__ void k_wall_init(const uint8_t* __restrict__ solid, uint8_t* __restrict__ d, size_t n) {

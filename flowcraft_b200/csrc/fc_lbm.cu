@@ -60,6 +60,7 @@ struct fc_lbm {
     bool closure_on = false;  // learned closure in place of Smagorinsky
     fc::ClosureDev closure{};
     uint4* d_closure = nullptr;
+    uint4* d_closure_tc = nullptr;  // the weight image of the tensor-core MLP
     uint8_t* d_wall = nullptr;
     float* d_stage = nullptr;
     float* h_stage = nullptr;
@@ -215,6 +216,7 @@ void release(fc_lbm* h) {
     dfree(h->d_aero_partials);
     dfree(h->d_aero_result);
     dfree(h->d_closure);
+    dfree(h->d_closure_tc);
     dfree(h->d_wall);
     dfree(h->d_aa_bz);
     dfree(h->d_aa_outm);
@@ -396,7 +398,8 @@ cudaError_t launch_bulk(fc_lbm* h, const fc::StepParams& p, const void* fin, voi
                                   h->cur, aa_side(h));
     if (h->closure_on)
         return fc::launch_bulk_pull_learned(h->q, h->storage, fin, fout, h->d_bulk_bits, h->g, p, z0, zc,
-                                            h->d_diverged, s, nl, h->closure);
+                                            h->d_diverged, s, nl, h->closure,
+                                            (h->flags & FC_OPTION_TC_CLOSURE) ? 1 : 0);
     return fc::launch_bulk_pull(h->q, h->storage, fin, fout, h->d_bulk_bits, h->g, p, z0, zc, h->d_diverged, s, nl,
                                 (h->flags & FC_OPTION_TMA_STAGING) ? 1 : 0);
 }
@@ -826,15 +829,22 @@ int fc_lbm_set_closure(fc_lbm* h, const fc_closure* c) {
         }
     }
     if (!h->d_closure) FC_TRY(h, cudaMalloc(&h->d_closure, fc::kClosureVec * sizeof(uint4)), "alloc closure");
+    if (!h->d_closure_tc) FC_TRY(h, cudaMalloc(&h->d_closure_tc, fc::kTcWeightBytes), "alloc closure");
     std::vector<uint4> frag(fc::kClosureVec);
     fc::pack_closure(c->w1, c->b1, c->w2, c->b2, c->w3, c->b3, c->out_scale, frag.data());
+    std::vector<uint4> tcw(fc::kTcWeightBytes / sizeof(uint4));
+    fc::pack_closure_tc(c->w1, c->b1, c->w2, c->b2, c->w3, c->out_scale, reinterpret_cast<uint8_t*>(tcw.data()));
     // ordered after any step already queued on the solver's stream
     FC_TRY(h, cudaMemcpyAsync(h->d_closure, frag.data(), frag.size() * sizeof(uint4), cudaMemcpyHostToDevice,
                               h->stream),
            "upload closure");
+    FC_TRY(h, cudaMemcpyAsync(h->d_closure_tc, tcw.data(), fc::kTcWeightBytes, cudaMemcpyHostToDevice, h->stream),
+           "upload closure");
     FC_RC(wait_stream(h, kTransferTimeoutMs));
     fc::ClosureDev cd{};
     cd.frag = h->d_closure;
+    cd.tcw = h->d_closure_tc;
+    cd.b3 = c->b3 * c->out_scale;  // as the fragment image folds it
     cd.wall = h->d_wall;
     for (int k = 0; k < FC_CLOSURE_INPUTS; ++k) {
         cd.mean[k] = c->mean[k];

@@ -89,8 +89,15 @@ constexpr int kClosureGroups = 8;
 constexpr int kClosureVec = kClosureGroups * 32;  // uint4 entries
 constexpr int kWallFar = 255;                     // wall-distance byte for 15.94+ cells
 
+// Bytes of the closure's weight image for the tensor-core MLP (closure_tc.cuh):
+// W1 (32 x 16), W2 (32 x 32), the b2 block (32 x 16) and W3 (16 x 32), BF16,
+// each K-major in 8-row x 16-byte core matrices.
+constexpr int kTcWeightBytes = 5120;
+
 struct ClosureDev {
     const uint4* frag;    // kClosureVec entries
+    const uint4* tcw;     // kTcWeightBytes: the weight image of the tensor-core MLP
+    float b3;             // output bias, out_scale folded in
     const uint8_t* wall;  // per-cell wall distance, 1/16-cell steps
     float mean[kClosureIn];
     float inv_std[kClosureIn];
@@ -103,6 +110,10 @@ struct ClosureDev {
 // entries: BF16 weights and hidden-layer biases, FP32 output bias.
 void pack_closure(const float* w1, const float* b1, const float* w2, const float* b2, const float* w3, float b3,
                   float out_scale, uint4* out);
+// Host: the same weights (the same BF16 values) as the tensor-core MLP's
+// shared-memory image, kTcWeightBytes bytes into `out`.
+void pack_closure_tc(const float* w1, const float* b1, const float* w2, const float* b2, const float* w3,
+                     float out_scale, uint8_t* out);
 // Chamfer distance (in 1/16 cells, capped at kWallFar) from every cell to the
 // nearest solid cell; `tmp` is a scratch array of g.n bytes.
 cudaError_t launch_wall_distance(const uint8_t* solid, const Geom& g, uint8_t* out, uint8_t* tmp, cudaStream_t s);
@@ -115,9 +126,11 @@ cudaError_t launch_wall_distance(const uint8_t* solid, const Geom& g, uint8_t* o
 int closure_samples(int q, int storage, const void* f, const uint8_t* solid, const Geom& fg, float tau_c,
                     float filter_width, float* out, int64_t capacity, int64_t* count, cudaStream_t s);
 
+// `tc`: the MLP on the tcgen05 tensor cores, once per block (closure_tc.cuh),
+// instead of the warp-level mma.sync MLP.
 cudaError_t launch_bulk_pull_learned(int q, int storage, const void* fin, void* fout, const uint32_t* bulk_bits,
                                      const Geom& g, const StepParams& p, int z0, int zc, int* diverged,
-                                     cudaStream_t s, int* launched, const ClosureDev& cl);
+                                     cudaStream_t s, int* launched, const ClosureDev& cl, int tc = 0);
 cudaError_t launch_closure_probe(int q, int storage, const void* f, const uint8_t* solid, const Geom& g,
                                  const ClosureDev& cl, float* out, uint8_t* in_range, unsigned long long* counts,
                                  int layout, cudaStream_t s);

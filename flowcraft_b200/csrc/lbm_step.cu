@@ -22,6 +22,7 @@
 // they are independent and touch disjoint cells.
 #include "aa.cuh"
 #include "closure.cuh"
+#include "closure_tc.cuh"
 #include "collide.cuh"
 #include "collide2.cuh"
 #include "lbm_internal.h"
@@ -443,6 +444,121 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned(const 
     gr.x = la ? (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.x, p.tau))) * 4.5f : sga;
     gr.y = lb ? (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.y, p.tau))) * 4.5f : sgb;
     relax2<Q>(v, mr, gr);
+    if (bad) atomicOr(diverged, 1);
+    store_pair<Q, S>(pp, c, v, pair);
+}
+
+// k_bulk_pairs_learned with the MLP on the tcgen05 tensor cores
+// (FC_OPTION_TC_CLOSURE): the same loads, inputs, fallback and stores, but
+// the MLP runs once for the block's 512 cells (closure_cta_mlp), in blocks
+// where some cell is in the training range (a block-wide vote); the other
+// blocks relax with Smagorinsky at once. So no warp leaves before the vote:
+// rows past the lattice and lanes without a bulk pair load nothing or
+// in-lattice values and store nothing. Each block serializes its three
+// layers (MMA, commit, TMEM read-back, barrier), and with four blocks per SM
+// nothing hides those waits: in a developed flow this kernel takes twice the
+// time of the warp-level one, which stays the default.
+template <int Q, class S>
+__global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned_tc(const typename S::T* __restrict__ fin,
+                                                                           typename S::T* __restrict__ fout,
+                                                                           const uint32_t* __restrict__ bulk_bits,
+                                                                           Geom g, StepParams p, PlanePtrs pp, int z0,
+                                                                           int* __restrict__ diverged, ClosureDev cl) {
+    static_assert(!S::kExact, "the learned closure runs on the 16-bit offset formats");
+    using L = Lattice<Q>;
+    using T = typename S::T;
+    __shared__ TcSmem tsm;
+    const int y = blockIdx.y * kBulkRows + threadIdx.y;
+    const int z = z0 + blockIdx.z;
+    const bool row_ok = y < g.ny;  // the whole warp: one row
+    const size_t row = (size_t)z * g.ny + (row_ok ? y : 0);
+    const int k = 2 * threadIdx.x;
+    const int w = 2 * blockIdx.x + (k >> 5);
+    const uint32_t bits = row_ok && w < g.wpr ? __ldg(bulk_bits + row * g.wpr + w) : 0u;
+    const int x = 64 * blockIdx.x + k;
+    unsigned pair = (bits >> (k & 31)) & 3u;
+    unsigned plane = 0;
+    if (x == 0) {
+        plane |= pair & 1u;
+        pair &= ~1u;
+    }
+    if (x + 1 == g.nx - 1) {
+        plane |= pair & 2u;
+        pair &= ~2u;
+    }
+    const uint32_t c = (uint32_t)(row * g.nx + x);
+    const bool face = (y == 0) | (y == g.ny - 1) | (z == 0) | (z == g.nz - 1);
+    if (plane) plane_cell<Q, S>(fin, fout, g, p, plane == 1u ? x : x + 1, plane == 1u ? c : (size_t)c + 1);
+    const bool va = pair & 1u, vb = pair & 2u;
+
+    // The load path is chosen per warp: off the Y/Z faces every lane takes
+    // the pure pair pull (every source of a row off the faces lies inside the
+    // lattice, also for the cells a lane does not store: the inlet / outlet
+    // cell of a row end and wall cells), the masked general path on the faces.
+    // Lanes beyond the row load their own row and store nothing.
+    const uint32_t cs = x < g.nx ? c : (uint32_t)(row * g.nx);
+    float2 v[Q];
+    if (!row_ok) {
+        static_for<0, Q>([&](auto I) { v[decltype(I)::value] = make_float2(0.0f, 0.0f); });
+    } else if (!face) {
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            const T* src = static_cast<const T*>(pp.src[i]);
+            v[i] = L::ex(i) == 0 ? S::raw2(S::ld2(src + cs))
+                                 : make_float2(S::raw(S::ld(src + cs)), S::raw(S::ld(src + cs + 1u)));
+        });
+    } else {
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            const int py = y - L::ey(i), pz = z - L::ez(i);
+            const bool oy = py < 0 || py >= g.ny;
+            const bool oz = pz < 0 || pz >= g.nz;
+            const bool out = oy || oz;
+            const int pl = out ? edge_plane<Q, i>(oy, oz, p) : i;
+            const uint32_t off = out ? 0u : (uint32_t)link_offset<Q>(i, g);
+            const uint32_t sa = va ? c - off : cs;
+            const uint32_t sb = vb ? c + 1u - off : cs + 1u;
+            const T* base = fin + (size_t)pl * g.n;
+            v[i] = make_float2(S::raw(S::ld(base + sa)), S::raw(S::ld(base + sb)));
+        });
+    }
+    Mom2 mo;
+    const unsigned bad = moments2<Q>(v, mo) & pair;
+    // The range test goes input by input, each stage only in warps where
+    // some lane is still in range (warp votes keep the branches uniform).
+    float ra, rb;
+    const float xa0 = closure_x0(mo.pp.x, mo.inv.x, ra), xb0 = closure_x0(mo.pp.y, mo.inv.y, rb);
+    bool la = row_ok && closure_x0_in_range(cl, xa0), lb = row_ok && closure_x0_in_range(cl, xb0);
+    float xa1 = 0.0f, xa2 = 0.0f, xb1 = 0.0f, xb2 = 0.0f;
+    if (__any_sync(0xffffffffu, la || lb)) {
+        closure_x12(mo.pxx.x, mo.pyy.x, mo.pzz.x, mo.pxy.x, mo.pxz.x, mo.pyz.x, ra, xa1, xa2);
+        closure_x12(mo.pxx.y, mo.pyy.y, mo.pzz.y, mo.pxy.y, mo.pxz.y, mo.pyz.y, rb, xb1, xb2);
+        la = la && closure_x12_in_range(cl, xa1, xa2);
+        lb = lb && closure_x12_in_range(cl, xb1, xb2);
+    }
+    // the Smagorinsky fallback only where some lane of the warp needs it
+    float sga = 0.0f, sgb = 0.0f;
+    if (__any_sync(0xffffffffu, !(la && lb))) {
+        sga = smagorinsky_g(mo.pp.x, mo.rho.x, mo.inv.x, p.tau, p.cs);
+        sgb = smagorinsky_g(mo.pp.y, mo.rho.y, mo.inv.y, p.tau, p.cs);
+    }
+    // A cell outside the training range takes the Smagorinsky value, so a
+    // block with no cell in range has no use for the MLP and skips it (the
+    // result is the same).
+    const bool live = __any_sync(0xffffffffu, la || lb);
+    float2 g2 = make_float2(sga, sgb);
+    if (__syncthreads_or(live)) {
+        // both cells' wall distances in one aligned load (x and nx are even)
+        const unsigned wd = pair ? (unsigned)__ldg(reinterpret_cast<const unsigned short*>(cl.wall + c)) : 0xffffu;
+        uint4 ia, ib;
+        closure_pack_inputs(cl, xa0, xa1, xa2, (float)(wd & 0xffu) * 0.0625f, reinterpret_cast<uint32_t*>(&ia));
+        closure_pack_inputs(cl, xb0, xb1, xb2, (float)(wd >> 8) * 0.0625f, reinterpret_cast<uint32_t*>(&ib));
+        const float2 nu = closure_cta_mlp(tsm, cl, ia, ib, live, diverged);
+        if (la) g2.x = (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.x, p.tau))) * 4.5f;
+        if (lb) g2.y = (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.y, p.tau))) * 4.5f;
+    }
+    if (!pair) return;
+    relax2<Q>(v, mo, g2);
     if (bad) atomicOr(diverged, 1);
     store_pair<Q, S>(pp, c, v, pair);
 }
@@ -950,7 +1066,7 @@ static cudaError_t boundary_t(const void* fin, void* fout, const BoundaryList& b
 template <int Q, class S>
 static cudaError_t bulk_learned_t(const void* fin, void* fout, const uint32_t* bits, const Geom& g,
                                   const StepParams& p, int z0, int zc, int* dv, cudaStream_t s, int* launched,
-                                  const ClosureDev& cl) {
+                                  const ClosureDev& cl, int tc) {
     *launched = 0;
     if constexpr (S::kExact) {
         return cudaErrorNotSupported;
@@ -966,8 +1082,12 @@ static cudaError_t bulk_learned_t(const void* fin, void* fout, const uint32_t* b
         }
         dim3 block(32, kBulkRows, 1);
         dim3 grid((unsigned)((g.nx + 63) / 64), (unsigned)((g.ny + kBulkRows - 1) / kBulkRows), (unsigned)zc);
-        k_bulk_pairs_learned<Q, S><<<grid, block, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout, bits, g,
-                                                          p, pp, z0, dv, cl);
+        if (tc)
+            k_bulk_pairs_learned_tc<Q, S><<<grid, block, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout,
+                                                                 bits, g, p, pp, z0, dv, cl);
+        else
+            k_bulk_pairs_learned<Q, S><<<grid, block, 0, s>>>((const typename S::T*)fin, (typename S::T*)fout, bits,
+                                                              g, p, pp, z0, dv, cl);
         ++*launched;
         return cudaGetLastError();
     }
@@ -1032,8 +1152,8 @@ cudaError_t launch_boundary_pull(int q, int storage, const void* fin, void* fout
 
 cudaError_t launch_bulk_pull_learned(int q, int storage, const void* fin, void* fout, const uint32_t* bulk_bits,
                                      const Geom& g, const StepParams& p, int z0, int zc, int* diverged,
-                                     cudaStream_t s, int* launched, const ClosureDev& cl) {
-    FC_DISPATCH(q, storage, bulk_learned_t, fin, fout, bulk_bits, g, p, z0, zc, diverged, s, launched, cl);
+                                     cudaStream_t s, int* launched, const ClosureDev& cl, int tc) {
+    FC_DISPATCH(q, storage, bulk_learned_t, fin, fout, bulk_bits, g, p, z0, zc, diverged, s, launched, cl, tc);
 }
 
 cudaError_t launch_boundary_pull_learned(int q, int storage, const void* fin, void* fout, const BoundaryList& bl,

@@ -73,6 +73,9 @@ class _Params(ctypes.Structure):
 # fc_options.flags: stage the interior rows in shared memory by TMA tensor
 # copies (16-bit formats; identical results, off by default)
 OPTION_TMA_STAGING = 1
+# fc_options.flags: the learned closure's MLP on the tcgen05 tensor cores,
+# once per block of the ping-pong bulk step (FC_OPTION_TC_CLOSURE)
+OPTION_TC_CLOSURE = 2
 
 
 class _Options(ctypes.Structure):

@@ -104,6 +104,14 @@ typedef struct fc_params {
  * results are identical. It is off by default: on B200 the direct loads are
  * faster (the step is issue-bound, not latency-bound). */
 #define FC_OPTION_TMA_STAGING 1
+/* TC_CLOSURE evaluates the learned closure's MLP in the ping-pong bulk step
+ * on the tcgen05 tensor cores, once per block of 512 cells (shared-memory
+ * operands, TMEM accumulators), instead of per warp with mma.sync. Results
+ * agree to the FP32 rounding of the accumulation. It is off by default:
+ * each block waits on its three layers in turn, and on B200 the step takes
+ * twice as long in a developed flow. The in-place (AA) learned step and the
+ * boundary list keep the warp-level MLP. */
+#define FC_OPTION_TC_CLOSURE 2
 
 typedef struct fc_options {
     int32_t device;    /* CUDA device ordinal */

@@ -143,6 +143,54 @@ def test_step_with_closure_vs_fp64_oracle(gpu, oracle_built, storage, tol, margi
     assert effect[:, 1:].max() > margin * d[:, 1:].max()
 
 
+@pytest.mark.parametrize("shape_idx", [0, 2])
+@pytest.mark.parametrize("storage,tol", [("FP16_OFFSET", 3e-4), ("BF16_OFFSET", 2e-3)])
+def test_tensor_core_closure(gpu, oracle_built, shape_idx, storage, tol):
+    """FC_OPTION_TC_CLOSURE: the bulk step's MLP once per block on the tcgen05
+    tensor cores. Against the warp-level MMA path it may differ only by the
+    FP32 rounding of the accumulation (a few storage steps after 40 steps),
+    and against the FP64 oracle running the same closure it keeps the
+    tolerance of the warp-level path. The 96 x 20 x 24 lattice has a block
+    row past the lattice and lanes past the row end."""
+    from flowcraft_b200.lbm import (LatticeModel, LbmSolver, OPTION_TC_CLOSURE, Params, Storage, Streaming,
+                                    VoxelGrid)
+    case = _shape_case(*SHAPES[shape_idx][1:], q=19)
+    probe = GpuAdapter(case, storage=Storage[storage])
+    probe.step(30)
+    cw = _weights(probe)
+    probe.s.close()
+    solid, sdf = geometry(case["geom"])
+    nz, ny, nx = solid.shape
+    p = case["params"]
+    prm = Params(tau=p["tau"], inletVelocity=p["inlet_velocity"], reverseFlow=bool(p.get("reverse_flow", 0)),
+                 freeSlipY=bool(p.get("free_slip_y", 1)), freeSlipZ=bool(p.get("free_slip_z", 1)),
+                 smagorinskyCs=p["smagorinsky_cs"])
+    sims = []
+    for flags in (OPTION_TC_CLOSURE, 0):
+        s = LbmSolver()
+        assert s.Init(0, VoxelGrid(nx, ny, nz, solid=solid, signedDistance=sdf), LatticeModel.D3Q19,
+                      Storage[storage], Streaming.PINGPONG, flags), s.LastError()
+        s.Reset(prm, case["seed_mid"])
+        s.SetClosure(cw)
+        sims.append(s)
+    assert sims[0].ClosureCoverage()["cells_in_range"] > 0
+    ref = OracleAdapter(case, "f64")
+    ref.o.set_closure(cw)
+    for s in sims:
+        s.Step(None, 40)
+    ref.step(40)
+    fl = ~solid.ravel().astype(bool)
+    g_tc, g_w = (s.ReadbackField().reshape(-1, 4).astype(np.float64) for s in sims)
+    r = ref.o.readback_field_f64().reshape(-1, 4)
+    d_w = np.abs(g_tc - g_w)[fl].max()
+    d_r = np.abs(g_tc - r)[fl].max()
+    print(f"{storage} {SHAPES[shape_idx][0]}: tcgen05 vs warp MMA max |d| {d_w:.2e}, vs FP64 oracle {d_r:.2e}")
+    assert np.isfinite(g_tc).all() and not sims[0].HasDiverged()
+    assert d_w < tol / 4 and d_r < tol
+    for s in sims:
+        s.close()
+
+
 def test_fallback_reproduces_smagorinsky(gpu):
     """With a training range no cell falls into, every cell keeps the
     Smagorinsky tau_eff. The learned kernels collide every cell on the stored
