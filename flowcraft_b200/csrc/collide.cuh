@@ -152,7 +152,7 @@ __device__ __forceinline__ bool collide_regularized(float (&f)[Q], float tau, fl
 namespace fc {
 
 // The same regularized + Smagorinsky collision, rearranged for throughput.
-// Used with the 16-bit storage formats, whose accuracy is judged against the
+// Used with the 16-bit storage formats, whose accuracy is measured against the
 // FP64 oracle rather than bit-for-bit; the FP32 format keeps
 // collide_regularized.
 //

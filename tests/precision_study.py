@@ -1,12 +1,14 @@
-"""Precision study (the SURVEY's config C2 at half size): the GPU storage
-formats and the learned closure against the FP64 oracle, and the learned
-closure's drag and lift against the FP32 Smagorinsky GPU run.
+"""Precision study (the 384x192x192 NACA 0012 precision configuration at
+half size): the GPU storage formats and the learned closure against the FP64
+oracle, and the learned closure's drag and lift against the FP32 Smagorinsky
+GPU run.
 
-Case: NACA 0012 wing, chord 48, span 64, 4 deg, on 192x96x96 (C2 halved, so
-nu and tau are C2's: U 0.06, Re 5e3 on the chord, tau 0.50173), Smagorinsky
-Cs 0.1, mid-speed seed, 1000 steps, D3Q19 and D3Q15. Drag and lift are the
-x and z sums of the solid cells' momentum-exchange force (the device FP64
-integral), normalized by 0.5 rho U^2 chord span.
+Case: NACA 0012 wing, chord 48, span 64, 4 deg, on 192x96x96 (the full-size
+case halved, so nu and tau are the full-size case's: U 0.06, Re 5e3 on the
+chord, tau 0.50173), Smagorinsky Cs 0.1, mid-speed seed, 1000 steps, D3Q19
+and D3Q15. Drag and lift are the x and z sums of the solid cells'
+momentum-exchange force (the device FP64 integral), normalized by
+0.5 rho U^2 chord span.
 
 Not collected by pytest; run on a GPU machine:  python tests/precision_study.py
 It prints one JSON object and a markdown table. Cd and Cl are reported at
