@@ -11,8 +11,9 @@
 //                     pair loads and stores in every direction); an odd step
 //                     pulls from the upstream cells and pushes to the
 //                     downstream ones (aligned pairs for e_x = 0, element
-//                     accesses otherwise). Face and row-end warps take the
-//                     general path with the edge and inlet / outlet rules.
+//                     accesses otherwise). Row-end warps take the same
+//                     loads plus the inlet / outlet rules; face warps take
+//                     the general path with the edge rules.
 //   k_boundary_aa     the boundary list. The Bouzidi far-side partner
 //                     f*_i(c), which the pulling cell c + e_i overwrites in
 //                     place, comes from the side buffer the entry itself
@@ -182,11 +183,20 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_aa(typename S:
     const bool edge = (blockIdx.x == 0) | (64 * (int)blockIdx.x + 64 >= g.nx);
 
     float2 v[Q];
-    if (!face && !edge) {
-        if (pair != 3u) {
+    if (!face) {
+        // Off the Y/Z faces every source slot of a row lies inside the set,
+        // also for a cell this lane does not store (the inlet / outlet cell of
+        // a row end, a wall cell), so row-end warps take the same loads; their
+        // partial pairs keep the masked pair collision of the ping-pong step.
+        if (pair != 3u && !edge) {
             aa_interior_cell<Q, S, Odd>(f, g, p, pair == 1u ? c : c + 1u, diverged);
             return;
         }
+        if (plane) {
+            const int px = plane == 1u ? x : x + 1;
+            aa_plane_cell<Q, S, Odd>(f, g, p, sd, px, y, z, plane == 1u ? c : c + 1u, row);
+        }
+        if (!pair) return;
         static_for<0, Q>([&](auto I) {
             constexpr int i = decltype(I)::value;
             const T* src = static_cast<const T*>(pp.src[i]);
@@ -204,25 +214,48 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_aa(typename S:
                     v[i] = make_float2(S::raw(ha), S::raw(hb));
             }
         });
-        if (collide_pair<Q, S>(v, p.tau, p.cs)) atomicOr(diverged, 1);
-        static_for<0, Q>([&](auto I) {
-            constexpr int i = decltype(I)::value;
-            T* dst = static_cast<T*>(pp.dst[i]);
-            T2 h;
-            if constexpr (S::kExact)
-                h = S::enc2(v[i].x, v[i].y, L::w(i));
-            else
-                h = S::pack2(v[i].x, v[i].y);
-            if (!Odd || L::ex(i) == 0) {
-                *reinterpret_cast<T2*>(dst + c) = h;
-            } else {
-                dst[c] = h.x;
-                dst[c + 1u] = h.y;
+        if (collide_pair<Q, S>(v, p.tau, p.cs) & pair) atomicOr(diverged, 1);
+        if (pair == 3u) {
+            static_for<0, Q>([&](auto I) {
+                constexpr int i = decltype(I)::value;
+                T* dst = static_cast<T*>(pp.dst[i]);
+                T2 h;
+                if constexpr (S::kExact)
+                    h = S::enc2(v[i].x, v[i].y, L::w(i));
+                else
+                    h = S::pack2(v[i].x, v[i].y);
+                if (!Odd || L::ex(i) == 0) {
+                    *reinterpret_cast<T2*>(dst + c) = h;
+                } else {
+                    dst[c] = h.x;
+                    dst[c + 1u] = h.y;
+                }
+            });
+        } else {  // a partial pair of a row-end warp: its valid cell only
+            static_for<0, Q>([&](auto I) {
+                constexpr int i = decltype(I)::value;
+                T* dst = static_cast<T*>(pp.dst[i]) + c;
+                T2 h;
+                if constexpr (S::kExact)
+                    h = S::enc2(v[i].x, v[i].y, L::w(i));
+                else
+                    h = S::pack2(v[i].x, v[i].y);
+                if (pair & 1u) dst[0] = h.x;
+                if (pair & 2u) dst[1] = h.y;
+            });
+        }
+        if (edge) {  // upstream-neighbour moments for the outlets of both flow directions
+            const int ca = (pair & 1u) ? outm_col(x, g) : -1, cb = (pair & 2u) ? outm_col(x + 1, g) : -1;
+            if (ca >= 0 || cb >= 0) {
+                float a[Q], b[Q];
+                pair_stored<Q, S>(v, a, b);
+                if (ca >= 0) sd.outm[outm_index(sd, Odd ? 0 : 1, ca, row)] = plain_moments<Q>(a);
+                if (cb >= 0) sd.outm[outm_index(sd, Odd ? 0 : 1, cb, row)] = plain_moments<Q>(b);
             }
-        });
+        }
         return;
     }
-    // general pair path (face rows, first / last chunk of a row)
+    // general pair path (face rows)
     if (plane) {
         const int px = plane == 1u ? x : x + 1;
         aa_plane_cell<Q, S, Odd>(f, g, p, sd, px, y, z, plane == 1u ? c : c + 1u, row);
@@ -364,9 +397,10 @@ __global__ void __launch_bounds__(128) k_boundary_aa(typename S::T* f, BoundaryL
 }
 
 // Stores of a cell pair after the collision (v: scaled offsets or full
-// floats, as collide_pair leaves them): the aligned form of the interior
-// full-pair path (fast), or the general masked form with the edge and
-// outlet-moment rules of the face / row-end path.
+// floats, as collide_pair leaves them): the aligned form for full pairs off
+// the faces (fast), or the general masked form with the edge and
+// outlet-moment rules (the cells feeding the outlet moments, x = 1 and
+// nx-2, always sit in partial pairs).
 template <int Q, class S, bool Odd>
 __device__ __forceinline__ void aa_store_pair(typename S::T* f, const PlanePtrs& pp, const Geom& g, const AaSide& sd,
                                               const float2 (&v)[Q], uint32_t c, int x, int y, int z, size_t row,
@@ -455,11 +489,15 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_aa_learned(typ
     const uint32_t c = (uint32_t)(row * g.nx + x);
     const uint32_t cs = x < g.nx ? c : (uint32_t)(row * g.nx);  // lanes past the row end read its first pair
     const bool face = (y == 0) | (y == g.ny - 1) | (z == 0) | (z == g.nz - 1);
-    const bool edge = (blockIdx.x == 0) | (64 * (int)blockIdx.x + 64 >= g.nx);
-    const bool fast = !face && !edge;
+    // off the faces every source slot lies inside the set (k_bulk_pairs_aa)
+    const bool fast = !face;
 
     float2 v[Q];
     if (fast) {
+        if (plane) {
+            const int px = plane == 1u ? x : x + 1;
+            aa_plane_cell<Q, S, Odd>(f, g, p, sd, px, y, z, plane == 1u ? c : c + 1u, row);
+        }
         static_for<0, Q>([&](auto I) {
             constexpr int i = decltype(I)::value;
             const T* src = static_cast<const T*>(pp.src[i]);
