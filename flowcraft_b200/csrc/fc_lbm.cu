@@ -510,6 +510,8 @@ int fc_lbm_init(fc_lbm* h, const fc_grid_desc* grid, int32_t model, const fc_opt
         return fail(h, FC_LBM_ERR_INVALID_ARG, "unknown storage format");
     if (o.streaming != FC_STREAMING_PINGPONG && o.streaming != FC_STREAMING_AA)
         return fail(h, FC_LBM_ERR_INVALID_ARG, "unknown streaming mode");
+    if (o.flags & ~(FC_OPTION_TMA_STAGING | FC_OPTION_TC_CLOSURE))
+        return fail(h, FC_LBM_ERR_INVALID_ARG, "unknown option flags");
     if (o.streaming == FC_STREAMING_AA && (grid->nx % 2 != 0 || grid->nx < 4))
         return fail(h, FC_LBM_ERR_UNSUPPORTED, "AA (in-place) streaming needs an even nx of at least 4");
     const size_t n = (size_t)grid->nx * (size_t)grid->ny * (size_t)grid->nz;

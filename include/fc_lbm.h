@@ -117,7 +117,7 @@ typedef struct fc_options {
     int32_t device;    /* CUDA device ordinal */
     int32_t storage;   /* FC_STORAGE_* */
     int32_t streaming; /* FC_STREAMING_* */
-    int32_t flags;     /* FC_OPTION_* bits, 0 for the defaults */
+    int32_t flags;     /* FC_OPTION_* bits, 0 for the defaults; other bits are rejected */
 } fc_options;
 
 /* LbmSolver::Stats (FlowCraft/LbmSolver.h:172-184) plus the FP64 sums the

@@ -94,3 +94,13 @@ def test_init_rejects_bad_grids(cuda_lib):
     assert "positive" in s.LastError()
     assert s.Init(0, VoxelGrid(2000, 2000, 1100, solid=np.zeros(1, np.uint8))) is False
     assert "2^32" in s.LastError()
+
+
+def test_init_rejects_unknown_option_flags(cuda_lib):
+    from flowcraft_b200.lbm import OPTION_TC_CLOSURE, OPTION_TMA_STAGING, LbmSolver, Storage, Streaming, VoxelGrid
+    s = LbmSolver()
+    g = VoxelGrid(8, 4, 4, solid=np.zeros(128, np.uint8))
+    bad = (OPTION_TMA_STAGING | OPTION_TC_CLOSURE) << 1
+    assert s.Init(0, g, storage=Storage.FP16_OFFSET, streaming=Streaming.PINGPONG, flags=bad) is False
+    assert "option flags" in s.LastError()
+    assert not s.IsValid()
