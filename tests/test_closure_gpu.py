@@ -143,18 +143,18 @@ def test_step_with_closure_vs_fp64_oracle(gpu, oracle_built, storage, tol, margi
     assert effect[:, 1:].max() > margin * d[:, 1:].max()
 
 
-@pytest.mark.parametrize("shape_idx", [0, 2])
+@pytest.mark.parametrize("shape_idx,q", [(0, 19), (2, 19), (0, 15)])
 @pytest.mark.parametrize("storage,tol", [("FP16_OFFSET", 3e-4), ("BF16_OFFSET", 2e-3)])
-def test_tensor_core_closure(gpu, oracle_built, shape_idx, storage, tol):
+def test_tensor_core_closure(gpu, oracle_built, shape_idx, q, storage, tol):
     """FC_OPTION_TC_CLOSURE: the bulk step's MLP once per block on the tcgen05
-    tensor cores. Against the warp-level MMA path it may differ only by the
-    FP32 rounding of the accumulation (a few storage steps after 40 steps),
-    and against the FP64 oracle running the same closure it keeps the
-    tolerance of the warp-level path. The 96 x 20 x 24 lattice has a block
-    row past the lattice and lanes past the row end."""
+    tensor cores. The same BF16 operands and the same FP32 accumulation give
+    the warp-level MMA path's results bit for bit, and against the FP64
+    oracle running the same closure it keeps the tolerance of the warp-level
+    path. The 96 x 20 x 24 lattice has a block row past the lattice and lanes
+    past the row end."""
     from flowcraft_b200.lbm import (LatticeModel, LbmSolver, OPTION_TC_CLOSURE, Params, Storage, Streaming,
                                     VoxelGrid)
-    case = _shape_case(*SHAPES[shape_idx][1:], q=19)
+    case = _shape_case(*SHAPES[shape_idx][1:], q=q)
     probe = GpuAdapter(case, storage=Storage[storage])
     probe.step(30)
     cw = _weights(probe)
@@ -168,8 +168,9 @@ def test_tensor_core_closure(gpu, oracle_built, shape_idx, storage, tol):
     sims = []
     for flags in (OPTION_TC_CLOSURE, 0):
         s = LbmSolver()
-        assert s.Init(0, VoxelGrid(nx, ny, nz, solid=solid, signedDistance=sdf), LatticeModel.D3Q19,
-                      Storage[storage], Streaming.PINGPONG, flags), s.LastError()
+        assert s.Init(0, VoxelGrid(nx, ny, nz, solid=solid, signedDistance=sdf),
+                      LatticeModel.D3Q19 if q == 19 else LatticeModel.D3Q15, Storage[storage], Streaming.PINGPONG,
+                      flags), s.LastError()
         s.Reset(prm, case["seed_mid"])
         s.SetClosure(cw)
         sims.append(s)
@@ -184,9 +185,12 @@ def test_tensor_core_closure(gpu, oracle_built, shape_idx, storage, tol):
     r = ref.o.readback_field_f64().reshape(-1, 4)
     d_w = np.abs(g_tc - g_w)[fl].max()
     d_r = np.abs(g_tc - r)[fl].max()
-    print(f"{storage} {SHAPES[shape_idx][0]}: tcgen05 vs warp MMA max |d| {d_w:.2e}, vs FP64 oracle {d_r:.2e}")
+    print(f"{storage} D3Q{q} {SHAPES[shape_idx][0]}: tcgen05 vs warp MMA max |d| {d_w:.2e}, "
+          f"vs FP64 oracle {d_r:.2e}")
     assert np.isfinite(g_tc).all() and not sims[0].HasDiverged()
-    assert d_w < tol / 4 and d_r < tol
+    assert np.array_equal(g_tc.astype(np.float32).view(np.uint32), g_w.astype(np.float32).view(np.uint32))
+    assert np.array_equal(sims[0].SavePopulations().view(np.uint32), sims[1].SavePopulations().view(np.uint32))
+    assert d_r < tol
     for s in sims:
         s.close()
 
