@@ -495,7 +495,9 @@ def run_ours(args, cfg, rank, world, local_rank):
         "traffic": trf * head["bulk_cells"] if trf else None,
         "kernel": kernel_of(head["variant"]) + " (all bulk-mask cells)",
         "algorithmic_bytes_per_launch": head["bulk_bytes_per_launch"],
-        "peak_source": f"{peak_src} ({'MEASURED_PEAKS.json hbm_gbs' if peak_src == 'measured' else 'fallback'})",
+        "peak_source": ("measured: MEASURED_PEAKS.json hbm_gbs" if peak_src == "measured"
+                        else f"fallback: {FALLBACK_HBM_GBS:.0f} GB/s, an earlier copy measurement on this GPU type "
+                             "(no MEASURED_PEAKS.json)"),
     }
     e2e = None
     if not args.no_e2e:
