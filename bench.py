@@ -397,9 +397,8 @@ def run_e2e(args, cfg, solid, sdf, variant, dev_index):
     s.ReadbackFieldRange(0, cfg["nz"], out)
     el = time.perf_counter() - t0
     s.close()
-    layer = cfg["nx"] * cfg["ny"] * 16
     h2d = n * (1 + 4)
-    d2h = layer * steps + n * 16 + 96
+    d2h = 4 * steps + n * 16 + 96  # the probe's verdict flag per step, the stats, the field
     return {"value": n * steps / el / 1e9, "unit": "GLUPS", "seconds": el, "steps": steps,
             "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps,
             "diverged": diverged, "avg_density": stats.avgDensity,

@@ -967,33 +967,17 @@ int fc_lbm_probe_slice_health(fc_lbm* h, int32_t z, int32_t* diverged) {
     DeviceGuard dg(h->device);
     const int gz = std::min(std::max(z, 0), h->g.nz - 1);  // LbmSolver.cpp:655
     const size_t layer = (size_t)h->g.nxy;
-    const size_t c0 = (size_t)gz * layer;
-    *diverged = 0;
-    const size_t chunk = h->stage_floats / 4;
-    for (size_t done = 0; done < layer; done += chunk) {
-        const size_t nc = std::min(chunk, layer - done);
-        FC_TRY(h, fc::launch_field(h->q, h->storage, h->pop[h->cur], h->d_solid, h->d_sdf, h->g, c0 + done, nc,
-                                   h->d_stage, layout_of(h), h->stream),
-               "field kernel");
-        h->launches++;
-        FC_TRY(h, cudaMemcpyAsync(h->h_stage, h->d_stage, nc * 4 * sizeof(float), cudaMemcpyDeviceToHost, h->stream),
-               "layer download");
-        FC_RC(wait_stream(h, kTransferTimeoutMs));
-        for (size_t i = 0; i < nc; ++i) {  // LbmSolver.cpp:699-716
-            const float* v = h->h_stage + i * 4;
-            if (!std::isfinite(v[0]) || !std::isfinite(v[1]) || !std::isfinite(v[2]) || !std::isfinite(v[3])) {
-                *diverged = 1;
-                return FC_LBM_OK;
-            }
-            if (!h->solid_cpu[c0 + done + i]) {
-                const float sp2 = v[1] * v[1] + v[2] * v[2] + v[3] * v[3];
-                if (v[0] <= 0.0f || sp2 > 4.0f) {
-                    *diverged = 1;
-                    return FC_LBM_OK;
-                }
-            }
-        }
-    }
+    // the layer's field values and the reference's checks on them
+    // (LbmSolver.cpp:699-716), evaluated on the device: one flag comes back
+    int* d_flag = reinterpret_cast<int*>(h->d_stage);
+    FC_TRY(h, cudaMemsetAsync(d_flag, 0, sizeof(int), h->stream), "clear probe flag");
+    FC_TRY(h, fc::launch_probe_health(h->q, h->storage, h->pop[h->cur], h->d_solid, h->d_sdf, h->g,
+                                      (size_t)gz * layer, layer, d_flag, layout_of(h), h->stream),
+           "probe kernel");
+    h->launches++;
+    FC_TRY(h, cudaMemcpyAsync(h->h_stage, d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "probe download");
+    FC_RC(wait_stream(h, kTransferTimeoutMs));
+    *diverged = *reinterpret_cast<const int*>(h->h_stage) != 0 ? 1 : 0;
     return FC_LBM_OK;
 }
 

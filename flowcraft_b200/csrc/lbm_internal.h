@@ -226,6 +226,10 @@ cudaError_t launch_seed_field(int q, int storage, void* f, const Geom& g, const 
 
 cudaError_t launch_field(int q, int storage, const void* f, const uint8_t* solid, const float* sdf, const Geom& g,
                          size_t cell0, size_t cells, float* out, int layout, cudaStream_t s);
+// ProbeSliceHealth's verdict for cells [cell0, cell0 + cells) on the device:
+// *flag (device, cleared by the caller) becomes nonzero if a cell fails.
+cudaError_t launch_probe_health(int q, int storage, const void* f, const uint8_t* solid, const float* sdf,
+                                const Geom& g, size_t cell0, size_t cells, int* flag, int layout, cudaStream_t s);
 cudaError_t launch_pops_out(int q, int storage, const void* f, const uint8_t* solid, int solid_is_weight,
                             const Geom& g, size_t cell0, size_t cells, float* out, int layout, cudaStream_t s);
 cudaError_t launch_pops_in(int q, int storage, void* f, const Geom& g, size_t cell0, size_t cells,

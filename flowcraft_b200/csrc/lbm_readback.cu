@@ -118,6 +118,37 @@ __global__ void __launch_bounds__(256) k_field(const typename S::T* __restrict__
                       : fluid_moments<Q, S>(f, g, c, x, y, z, layout);
 }
 
+// ProbeSliceHealth's verdict on the device (LbmSolver.cpp:699-716): the
+// field values k_field gives for cells [cell0, cell0 + cells), then every
+// value finite, and for fluid cells rho > 0 and |u|^2 <= 4 (the same float
+// operations as the host check). Any failing cell sets *flag.
+template <int Q, class S, int Lay>
+__global__ void __launch_bounds__(256) k_probe_health(const typename S::T* __restrict__ f,
+                                                       const uint8_t* __restrict__ solid, const float* __restrict__ sdf,
+                                                       Geom g, size_t cell0, size_t cells, int* __restrict__ flag,
+                                                       int layout_in) {
+    const int layout = Lay;
+    (void)layout_in;
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool bad = false;
+    if (k < cells) {
+        const size_t c = cell0 + k;
+        const int z = (int)(c / (size_t)g.nxy);
+        const size_t rem = c - (size_t)z * g.nxy;
+        const int y = (int)(rem / g.nx);
+        const int x = (int)(rem - (size_t)y * g.nx);
+        const bool sc = solid[c] != 0;
+        const float4 v = sc ? solid_force<Q, S>(f, solid, sdf, g, x, y, z, c, layout)
+                            : fluid_moments<Q, S>(f, g, c, x, y, z, layout);
+        bad = !isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z) || !isfinite(v.w);
+        if (!bad && !sc) {
+            const float sp2 = v.y * v.y + v.z * v.z + v.w * v.w;
+            bad = v.x <= 0.0f || sp2 > 4.0f;
+        }
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
 template <int Q, class S, int Lay>
 __global__ void k_pops_out(const typename S::T* __restrict__ f, const uint8_t* __restrict__ solid,
                            int solid_is_weight, Geom g, size_t cell0, size_t cells, float* __restrict__ out,
@@ -494,6 +525,15 @@ static cudaError_t field_t(const void* f, const uint8_t* solid, const float* sdf
 }
 
 template <int Q, class S>
+static cudaError_t probe_health_t(const void* f, const uint8_t* solid, const float* sdf, const Geom& g, size_t cell0,
+                                  size_t cells, int* flag, int layout, cudaStream_t s) {
+    if (cells == 0) return cudaSuccess;
+    FC_LAYOUT_LAUNCH(k_probe_health, (unsigned)((cells + 255) / 256), 256, (const typename S::T*)f, solid, sdf, g,
+                     cell0, cells, flag, layout);
+    return cudaGetLastError();
+}
+
+template <int Q, class S>
 static cudaError_t pops_out_t(const void* f, const uint8_t* solid, int sw, const Geom& g, size_t cell0, size_t cells,
                               float* out, int layout, cudaStream_t s) {
     if (cells == 0) return cudaSuccess;
@@ -537,6 +577,11 @@ static cudaError_t stats_t(const void* f, const uint8_t* solid, const float* sdf
 cudaError_t launch_field(int q, int storage, const void* f, const uint8_t* solid, const float* sdf, const Geom& g,
                          size_t cell0, size_t cells, float* out, int layout, cudaStream_t s) {
     FC_DISPATCH(q, storage, field_t, f, solid, sdf, g, cell0, cells, out, layout, s);
+}
+
+cudaError_t launch_probe_health(int q, int storage, const void* f, const uint8_t* solid, const float* sdf,
+                                const Geom& g, size_t cell0, size_t cells, int* flag, int layout, cudaStream_t s) {
+    FC_DISPATCH(q, storage, probe_health_t, f, solid, sdf, g, cell0, cells, flag, layout, s);
 }
 
 cudaError_t launch_pops_out(int q, int storage, const void* f, const uint8_t* solid, int solid_is_weight,

@@ -161,6 +161,35 @@ def test_reset_from_field_mismatch_is_ignored(gpu):
     assert np.array_equal(sim.readback_field(), before)
 
 
+@pytest.mark.parametrize("storage", ["FP32", "FP16_OFFSET"])
+def test_probe_verdict_matches_host_check_of_the_field(gpu, storage):
+    """ProbeSliceHealth evaluates the reference's checks (LbmSolver.cpp:699-716)
+    on the device. Its verdict for every layer must equal those checks run on
+    the host over the read-back field: any value not finite, or a fluid cell
+    with rho <= 0 or |u|^2 > 4. The state is seeded with a NaN density, an
+    excess speed and a negative density in three different layers."""
+    from flowcraft_b200.lbm import Storage
+    case = CASES["sphere48_q19"]
+    sim = GpuAdapter(case, storage=Storage[storage])
+    sim.step(5)
+    nz, ny, nx = geometry(case["geom"])[0].shape
+    solid = geometry(case["geom"])[0].reshape(nz, ny * nx).astype(bool)
+    field = sim.readback_field().reshape(nz, ny * nx, 4).copy()
+    fluid_y = np.nonzero(~solid[10])[0]
+    field[10, fluid_y[5], 0] = np.nan
+    field[12, fluid_y[7], 1:4] = (1.5, 1.0, 0.5)  # |u|^2 = 3.5: inside the bound
+    field[13, fluid_y[9], 1:4] = (1.6, 1.2, 0.6)  # |u|^2 = 4.36
+    field[15, fluid_y[11], 0] = -0.5
+    sim.reset_from_field(field.ravel())
+    got = sim.readback_field().reshape(nz, ny * nx, 4)
+    for z in range(nz):
+        v = got[z]
+        sp2 = (v[:, 1] * v[:, 1] + v[:, 2] * v[:, 2]) + v[:, 3] * v[:, 3]
+        want = (not np.isfinite(v).all()) or bool(np.any(~solid[z] & ((v[:, 0] <= 0) | (sp2 > 4.0))))
+        assert sim.s.ProbeSliceHealth(z) is want, z
+    assert [sim.s.ProbeSliceHealth(z) for z in (10, 12, 13, 15)] == [True, False, True, True]
+
+
 def test_divergence_detection_from_host_injected_state(gpu, oracle_built):
     """Failure detection without a GPU fault: host-prepared fields with a NaN
     cell, and with a 3x3x3 block at negative density, are seeded through
