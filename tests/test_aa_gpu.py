@@ -176,6 +176,28 @@ def test_aa_learned_closure_bit_identical_to_pingpong(gpu, name, storage):
     _compare(pp, aa, f"{name} learned after 18 steps")
 
 
+def test_aa_learned_ignores_the_tensor_core_option(gpu):
+    """FC_OPTION_TC_CLOSURE applies to the ping-pong bulk step; in place the
+    learned step keeps the warp-level MLP, so the flag changes nothing."""
+    from flowcraft_b200.lbm import (LatticeModel, LbmSolver, OPTION_TC_CLOSURE, Params, Storage, Streaming,
+                                    VoxelGrid)
+    case = BRANCHES["wide_q15"]
+    ref = Sim(case, "FP16_OFFSET")
+    cw = _closure_for(ref, 7)
+    ref.s.SetClosure(cw)
+    solid, sdf = geometry(case["geom"])
+    nz, ny, nx = solid.shape
+    s = LbmSolver()
+    assert s.Init(0, VoxelGrid(nx, ny, nz, solid=solid, signedDistance=sdf), LatticeModel.D3Q15,
+                  Storage.FP16_OFFSET, Streaming.AA, OPTION_TC_CLOSURE), s.LastError()
+    s.Reset(_params(case["params"]), case["seed_mid"])
+    s.SetClosure(cw)
+    ref.step(9)
+    s.Step(None, 9)
+    assert _same(ref.s.SavePopulations(), s.SavePopulations())
+    s.close()
+
+
 def test_aa_learned_step_range_chunks(gpu):
     """StepRange chunks in place with the closure equal whole steps."""
     case = BRANCHES["wide_q15"]
