@@ -1,0 +1,62 @@
+"""bench.py's variant routing on the CPU: each variant name maps to its
+storage format, streaming scheme, flow state, option flags, kernel name and
+committed ncu traffic figure. No GPU is used."""
+import os
+import sys
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+sys.path.insert(0, ROOT)
+
+import bench  # noqa: E402
+
+
+def test_variants_route_to_storage_streaming_and_kernel():
+    from flowcraft_b200 import Storage, Streaming
+    want = {
+        "fp16_learned": (Storage.FP16_OFFSET, Streaming.PINGPONG, "k_bulk_pairs_learned"),
+        "fp16_offset": (Storage.FP16_OFFSET, Streaming.PINGPONG, "k_bulk_pairs"),
+        "fp32": (Storage.FP32, Streaming.PINGPONG, "k_bulk_pairs"),
+        "fp16_aa": (Storage.FP16_OFFSET, Streaming.AA, "k_bulk_pairs_aa"),
+        "fp32_aa": (Storage.FP32, Streaming.AA, "k_bulk_pairs_aa"),
+        "fp16_aa_learned": (Storage.FP16_OFFSET, Streaming.AA, "k_bulk_pairs_aa_learned"),
+        "fp16_tc_learned": (Storage.FP16_OFFSET, Streaming.PINGPONG, "k_bulk_pairs_learned_tc"),
+        "fp16_tma": (Storage.FP16_OFFSET, Streaming.PINGPONG, "k_bulk_pairs"),
+    }
+    for v, (st, sm, kern) in want.items():
+        assert bench.storage_of(v) == st, v
+        assert bench.streaming_of(v) == sm, v
+        assert bench.kernel_of(v) == f"{kern}<19,{v}>", v
+        assert v in bench.BYTES_PER_ELEM, v
+
+
+def test_default_variants_are_known_and_headline_is_learned():
+    args = bench.parse_args([])
+    variants = args.variants.split(",")
+    assert variants[0] == "fp16_learned"
+    for v in variants:
+        bench.storage_of(v)
+        assert v in bench.BYTES_PER_ELEM
+    assert args.spinup > 0 and args.warmup >= 3
+
+
+def test_spinup_applies_to_learned_variants_only():
+    args = bench.parse_args(["--spinup", "123"])
+    assert bench.spinup_of(args, "fp16_learned") == 123
+    assert bench.spinup_of(args, "fp16_aa_learned") == 123
+    assert bench.spinup_of(args, "fp16_offset") == 0
+    assert bench.spinup_of(args, "fp32_aa") == 0
+
+
+def test_bytes_per_cell_update():
+    for v, elem in bench.BYTES_PER_ELEM.items():
+        per_cell = 19 * 2 * elem + bench.EXTRA_BYTES.get(v, 0)
+        assert per_cell == (152 if elem == 4 else 76) + (1 if v.endswith("_learned") else 0), v
+
+
+def test_committed_traffic_figures_are_read():
+    early = bench.ncu_traffic_per_cell("fp16_learned")
+    developed = bench.ncu_traffic_per_cell("fp16_learned", developed=True)
+    plain = bench.ncu_traffic_per_cell("fp16_offset")
+    assert early and developed and plain
+    for t in (early, developed, plain):
+        assert 70.0 < t < 80.0  # about the 76-77 algorithmic bytes per cell
