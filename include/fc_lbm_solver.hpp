@@ -25,6 +25,9 @@ namespace fc {
 enum class LatticeModel { D3Q15 = FC_LATTICE_D3Q15, D3Q19 = FC_LATTICE_D3Q19 };
 
 enum class Storage { FP32 = FC_STORAGE_FP32, FP16Offset = FC_STORAGE_FP16_OFFSET, BF16Offset = FC_STORAGE_BF16_OFFSET };
+// PingPong keeps two population copies (the reference's scheme); InPlace one,
+// streamed with the AA pattern (bit-identical results, half the memory).
+enum class Streaming { PingPong = FC_STREAMING_PINGPONG, InPlace = FC_STREAMING_AA };
 
 struct Vec3f {
     float x = 0.0f, y = 0.0f, z = 0.0f;
@@ -62,7 +65,11 @@ public:
     LbmSolver& operator=(const LbmSolver&) = delete;
 
     template <class Grid>
-    bool Init(int device, const Grid& grid, LatticeModel model, Storage storage = Storage::FP32) {
+    // The reference's Init(device, grid, model); storage, streaming and the
+    // FC_OPTION_* flags are additions with the reference's behaviour as
+    // defaults.
+    bool Init(int device, const Grid& grid, LatticeModel model, Storage storage = Storage::FP32,
+              Streaming streaming = Streaming::PingPong, int32_t flags = 0) {
         fc_grid_desc d{};
         d.nx = grid.nx;
         d.ny = grid.ny;
@@ -76,7 +83,7 @@ public:
         // a missing or mis-sized SDF means plain bounce-back (LbmReference.cpp:162-166)
         d.signed_distance = grid.signedDistance.size() == cells ? grid.signedDistance.data() : nullptr;
         d.memory = FC_MEMORY_HOST;
-        fc_options o{device, (int32_t)storage, FC_STREAMING_PINGPONG, 0};
+        fc_options o{device, (int32_t)storage, (int32_t)streaming, flags};
         model_ = model;
         const bool ok = fc_lbm_init(h_, &d, (int32_t)model, &o) == FC_LBM_OK;
         if (ok) {
@@ -154,6 +161,9 @@ public:
         return d != 0;
     }
     bool Sync(int timeoutMs = -1) { return fc_lbm_sync(h_, timeoutMs) == FC_LBM_OK; }
+    // The learned sub-grid closure (an addition; nullptr returns to
+    // Smagorinsky). The weights are copied.
+    bool SetClosure(const fc_closure* closure) { return fc_lbm_set_closure(h_, closure) == FC_LBM_OK; }
 
     const std::vector<uint8_t>& SolidMask() const { return solidCpu_; }
     bool IsValid() const { return fc_lbm_is_valid(h_) != 0; }
