@@ -87,6 +87,8 @@ def parse_args(argv=None):
                          "*_tma: interior rows staged by TMA")
     ap.add_argument("--spinup", type=int, default=2000,
                     help="untimed steps from the seed before the warm-up of the learned variants (flow state)")
+    ap.add_argument("--batch-shape", default=None,
+                    help="c3 only: ROWSxMULT (e.g. 4x2, or 0x1 for per-member launches) instead of the autotuner")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -419,7 +421,12 @@ def run_batch(args, cfg, rank, world, local_rank):
     solvers = [m[0] for m in mem]
     cells = sum(s.CellCount() for s in solvers)
     b = LbmBatch(solvers)
-    tuned = b.Tune(4)
+    if args.batch_shape:
+        rows, mult = (int(v) for v in args.batch_shape.lower().split("x"))
+        b.Config(rows, mult)
+        tuned = {"rows": rows, "grid_mult": mult, "fixed": True}
+    else:
+        tuned = b.Tune(4)
     b.Step(2 * args.warmup)
     torch.cuda.synchronize()
     barrier_sync(dist_on)
@@ -460,7 +467,8 @@ def run_batch(args, cfg, rank, world, local_rank):
             "config": {"workload": cfg["desc"], "lattices": len(solvers), "cells": cells,
                        "sizes": [m[1]["nx"] for m in mem], "autotune": tuned,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-            "diverged": any(diverged), "gpu_launches": 2 * steps, "clocks": clocks,
+            "diverged": any(diverged), "gpu_launches": (2 if tuned["rows"] else len(solvers) + 1) * steps,
+            "clocks": clocks,
             "sequential": {"glups": world * cells * steps / (seq_ms / 1e3) / 1e9, "ms_per_step": seq_ms / steps,
                            "how": "the same lattices stepped one after another on one stream with LbmSolver.Step"}}
     print(json.dumps(line), flush=True)

@@ -1,6 +1,8 @@
 """Many lattices stepped together (``fc_lbm_batch_*`` in include/fc_lbm.h):
-one persistent bulk launch over the tiles of every member per step, pairs of
-steps replayed as a CUDA graph, block shape picked by an autotuner. The
+one persistent bulk launch over the tiles of every member per step (or each
+member's own bulk kernel, side by side, when the autotuner finds that
+faster), pairs of steps replayed as a CUDA graph, block shape picked by an
+autotuner. The
 members stay ordinary ``LbmSolver`` objects (readbacks, forces, SetParams);
 the batch only steps them, bit-identically to ``LbmSolver.Step``."""
 from __future__ import annotations
@@ -11,7 +13,9 @@ import numpy as np
 
 from .lbm import FC_LBM_OK, LbmError, load_library
 
-CANDIDATES = [(r, m) for r in (4, 8, 16) for m in (1, 2)]
+# the persistent launch's block shapes, then rows 0: every member's own bulk
+# kernel, run side by side on forked streams
+CANDIDATES = [(r, m) for r in (4, 8, 16) for m in (1, 2)] + [(0, 1)]
 
 
 class LbmBatch:
@@ -38,13 +42,15 @@ class LbmBatch:
 
     def Tune(self, steps: int = 10) -> dict:
         """Times the block shapes on real steps (each member advances by
-        6 * (steps + 2) steps, even steps rounded up) and keeps the fastest."""
+        len(CANDIDATES) * (steps + 2) steps, even steps rounded up) and keeps
+        the fastest."""
         r, m = ctypes.c_int32(), ctypes.c_int32()
         ms = (ctypes.c_float * len(CANDIDATES))()
         self._check(self._lib.fc_lbm_batch_tune(self._h, int(steps), ctypes.byref(r), ctypes.byref(m), ms),
                     "batch tune")
         return {"rows": r.value, "grid_mult": m.value,
-                "ms_per_step": {f"rows{c[0]}_x{c[1]}": float(ms[i]) for i, c in enumerate(CANDIDATES)}}
+                "ms_per_step": {(f"rows{c[0]}_x{c[1]}" if c[0] else "per_member"): float(ms[i])
+                                for i, c in enumerate(CANDIDATES)}}
 
     def close(self):
         if getattr(self, "_h", None):

@@ -1350,16 +1350,21 @@ struct fc_lbm_batch {
     std::vector<fc::BatchLattice> h_lat;
     unsigned long long total = 0;   // bulk work items
     unsigned long long btotal = 0;  // boundary-list entries
-    int rows = 8, mult = 1, grid = 0;
+    int rows = 8, mult = 1, grid = 0;  // rows 0: every member's own bulk launch
     cudaGraphExec_t exec = nullptr;
+    // forked streams of the per-member bulk launches (rows 0)
+    static constexpr int kFork = 4;
+    cudaStream_t fork[kFork] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[kFork] = {};
     std::vector<uint64_t> sig;  // member state the descriptors and the graph were built for
     std::string err;
 };
 
 namespace {
 
-constexpr int kBatchRows[3] = {4, 8, 16};
-constexpr int kBatchMult[2] = {1, 2};
+// The autotuner's candidates, in the order of fc_lbm_batch_tune's times: the
+// persistent launch's block shapes, then every member's own bulk kernel.
+constexpr int kBatchCand[FC_LBM_BATCH_CANDIDATES][2] = {{4, 1}, {4, 2}, {8, 1}, {8, 2}, {16, 1}, {16, 2}, {0, 1}};
 
 int bfail(fc_lbm_batch* b, int code, const std::string& msg) {
     b->err = msg;
@@ -1429,15 +1434,16 @@ int batch_build(fc_lbm_batch* b) {
         bfirst += b1 > b0 ? b1 - b0 : 0;
         d.bits = h->d_bulk_bits;
         d.diverged = h->d_diverged;
+        const int rows = b->rows ? b->rows : 8;  // rows 0: the work-list is not used
         d.gx = (h->g.nx + 63) / 64;
-        d.gy = (h->g.ny + b->rows - 1) / b->rows;
+        d.gy = (h->g.ny + rows - 1) / rows;
         d.first = first;
         d.cur = h->cur;
         first += (unsigned long long)d.gx * d.gy * h->g.nz;
     }
     b->total = first;
     b->btotal = bfirst;
-    const int resident = fc::bulk_batch_resident(b->q, b->storage, b->rows);
+    const int resident = fc::bulk_batch_resident(b->q, b->storage, b->rows ? b->rows : 8);
     int sms = 0;
     FB_TRY(b, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device), "SM count");
     if (resident <= 0) return bfail(b, FC_LBM_ERR_CUDA, "batch kernel occupancy query failed");
@@ -1448,11 +1454,39 @@ int batch_build(fc_lbm_batch* b) {
     return FC_LBM_OK;
 }
 
+// Every member's own bulk kernel (the launch fc_lbm_step makes), spread over
+// the forked streams so that small lattices run side by side; joined back
+// into the batch stream. Under stream capture the fork and join become graph
+// dependencies.
+int batch_bulk_members(fc_lbm_batch* b, int parity) {
+    const int nf = (int)std::min<size_t>(fc_lbm_batch::kFork, b->m.size());
+    FB_TRY(b, cudaEventRecord(b->ev_fork, b->stream), "fork event");
+    for (int j = 0; j < nf; ++j) FB_TRY(b, cudaStreamWaitEvent(b->fork[j], b->ev_fork, 0), "fork");
+    cudaError_t e = cudaSuccess;
+    for (size_t k = 0; k < b->m.size() && e == cudaSuccess; ++k) {
+        fc_lbm* h = b->m[k];
+        if (h->n_bulk == 0) continue;
+        const int side = h->cur ^ parity;
+        int nl = 0;
+        e = launch_bulk(h, step_params(h), h->pop[side], h->pop[1 - side], 0, h->g.nz, b->fork[k % nf], &nl);
+    }
+    // always join, so that a capture can end
+    for (int j = 0; j < nf; ++j) {
+        const cudaError_t r = cudaEventRecord(b->ev_join[j], b->fork[j]);
+        const cudaError_t w = r == cudaSuccess ? cudaStreamWaitEvent(b->stream, b->ev_join[j], 0) : r;
+        if (e == cudaSuccess) e = w;
+    }
+    return bcuda(b, e, "batch member bulk step");
+}
+
 // One step of every member (parity relative to the members' current sets).
 int batch_step_direct(fc_lbm_batch* b, int parity) {
-    FB_TRY(b, fc::launch_bulk_batch(b->q, b->storage, b->rows, b->d_lat, (int)b->m.size(), b->total, parity, b->grid,
-                                    b->stream),
-           "batch bulk step");
+    if (b->rows == 0)
+        FC_RC(batch_bulk_members(b, parity));
+    else
+        FB_TRY(b, fc::launch_bulk_batch(b->q, b->storage, b->rows, b->d_lat, (int)b->m.size(), b->total, parity,
+                                        b->grid, b->stream),
+               "batch bulk step");
     FB_TRY(b, fc::launch_boundary_batch(b->q, b->storage, b->d_lat, (int)b->m.size(), b->btotal, parity, b->stream),
            "batch boundary step");
     return FC_LBM_OK;
@@ -1561,6 +1595,11 @@ int fc_lbm_batch_create(fc_lbm* const* members, int32_t count, fc_lbm_batch** ou
     DeviceGuard dg(b->device);
     cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+    for (int j = 0; j < fc_lbm_batch::kFork && e == cudaSuccess; ++j) {
+        e = cudaStreamCreateWithFlags(&b->fork[j], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join[j], cudaEventDisableTiming);
+    }
     if (e == cudaSuccess) e = cudaMalloc(&b->d_lat, (size_t)count * sizeof(fc::BatchLattice));
     if (e != cudaSuccess) {
         fc_lbm_batch_destroy(b);
@@ -1577,6 +1616,14 @@ void fc_lbm_batch_destroy(fc_lbm_batch* b) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->d_lat) cudaFree(b->d_lat);
     if (b->ev) cudaEventDestroy(b->ev);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    for (int j = 0; j < fc_lbm_batch::kFork; ++j) {
+        if (b->fork[j]) {
+            cudaStreamSynchronize(b->fork[j]);
+            cudaStreamDestroy(b->fork[j]);
+        }
+        if (b->ev_join[j]) cudaEventDestroy(b->ev_join[j]);
+    }
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
@@ -1598,8 +1645,8 @@ int fc_lbm_batch_step(fc_lbm_batch* b, int32_t n) {
 
 int fc_lbm_batch_config(fc_lbm_batch* b, int32_t rows, int32_t grid_mult) {
     if (!b) return FC_LBM_ERR_INVALID_ARG;
-    if ((rows != 4 && rows != 8 && rows != 16) || (grid_mult != 1 && grid_mult != 2))
-        return bfail(b, FC_LBM_ERR_INVALID_ARG, "rows must be 4, 8 or 16 and grid_mult 1 or 2");
+    if ((rows != 0 && rows != 4 && rows != 8 && rows != 16) || (grid_mult != 1 && grid_mult != 2))
+        return bfail(b, FC_LBM_ERR_INVALID_ARG, "rows must be 0, 4, 8 or 16 and grid_mult 1 or 2");
     b->rows = rows;
     b->mult = grid_mult;
     return FC_LBM_OK;
@@ -1619,29 +1666,29 @@ int fc_lbm_batch_tune(fc_lbm_batch* b, int32_t steps, int32_t* rows, int32_t* gr
     int rc = batch_enter(b);
     float best = 1e30f;
     int best_r = 8, best_m = 1, idx = 0;
-    for (int r : kBatchRows)
-        for (int mu : kBatchMult) {
-            if (rc != FC_LBM_OK) break;
-            b->rows = r;
-            b->mult = mu;
-            rc = batch_prepare(b, false);
-            for (int k = 0; k < 2 && rc == FC_LBM_OK; ++k) rc = batch_step_direct(b, k);  // warm-up
-            if (rc == FC_LBM_OK) rc = bcuda(b, cudaEventRecord(t0, b->stream), "timing");
-            for (int k = 0; k < timed && rc == FC_LBM_OK; ++k) rc = batch_step_direct(b, k & 1);
-            if (rc == FC_LBM_OK) rc = bcuda(b, cudaEventRecord(t1, b->stream), "timing");
-            if (rc == FC_LBM_OK) rc = batch_wait(b);
-            float ms = 0.0f;
-            if (rc == FC_LBM_OK) rc = bcuda(b, cudaEventElapsedTime(&ms, t0, t1), "timing");
-            const float per = ms / (float)timed;
-            if (ms_per_step) ms_per_step[idx] = per;
-            if (rc == FC_LBM_OK && per < best) {
-                best = per;
-                best_r = r;
-                best_m = mu;
-            }
-            ++idx;
-            batch_advance(b, timed + 2, 2);
+    for (const auto& cand : kBatchCand) {
+        const int r = cand[0], mu = cand[1];
+        if (rc != FC_LBM_OK) break;
+        b->rows = r;
+        b->mult = mu;
+        rc = batch_prepare(b, false);
+        for (int k = 0; k < 2 && rc == FC_LBM_OK; ++k) rc = batch_step_direct(b, k);  // warm-up
+        if (rc == FC_LBM_OK) rc = bcuda(b, cudaEventRecord(t0, b->stream), "timing");
+        for (int k = 0; k < timed && rc == FC_LBM_OK; ++k) rc = batch_step_direct(b, k & 1);
+        if (rc == FC_LBM_OK) rc = bcuda(b, cudaEventRecord(t1, b->stream), "timing");
+        if (rc == FC_LBM_OK) rc = batch_wait(b);
+        float ms = 0.0f;
+        if (rc == FC_LBM_OK) rc = bcuda(b, cudaEventElapsedTime(&ms, t0, t1), "timing");
+        const float per = ms / (float)timed;
+        if (ms_per_step) ms_per_step[idx] = per;
+        if (rc == FC_LBM_OK && per < best) {
+            best = per;
+            best_r = r;
+            best_m = mu;
         }
+        ++idx;
+        batch_advance(b, timed + 2, 2);
+    }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     b->rows = best_r;

@@ -640,11 +640,14 @@ __global__ void __launch_bounds__(128) k_closure_probe(const typename S::T* __re
 // tiles (64 x ROWS cells of one z layer) spanning every lattice of a batch.
 // Blocks stride over chunks of kBatchChunk consecutive tiles (block b takes
 // chunks b, b + G, b + 2G, ...), which interleaves cheap and costly tiles
-// across blocks. A block finds a tile's lattice by binary search over the
-// lattices' first items and keeps that lattice's descriptor (geometry, step
-// parameters, plane pointers) in shared memory while consecutive tiles stay
-// in it, so it reloads it at most once per chunk. The per-tile work and arithmetic are those of k_bulk_pairs, so
-// a batch step is bit-identical to stepping each lattice alone.
+// across blocks. A block's tiles only ever move forward, so it searches for
+// a tile's lattice (binary search over the lattices' first items) only when
+// the tile passes the end of the current one, and keeps that lattice's
+// descriptor (geometry, step parameters, plane pointers) in shared memory
+// meanwhile. The tile's (x chunk, row group, z) is divided out once per
+// chunk in 32-bit arithmetic and stepped from tile to tile after that. The
+// per-tile work and arithmetic are those of k_bulk_pairs, so a batch step is
+// bit-identical to stepping each lattice alone.
 template <int Q, class S, int ROWS>
 __global__ void __launch_bounds__(32 * ROWS, 32 / ROWS) k_bulk_pairs_batch(const BatchLattice* __restrict__ lat,
                                                                            int nlat, unsigned long long total,
@@ -653,23 +656,40 @@ __global__ void __launch_bounds__(32 * ROWS, 32 / ROWS) k_bulk_pairs_batch(const
     using T = typename S::T;
     __shared__ BatchLattice sl;
     const int tid = threadIdx.y * 32 + threadIdx.x;
-    int cur_lat = -1;
+    unsigned long long cur_end = 0;  // one past the current lattice's last tile
+    int bx = 0, ty = 0, z = 0;       // the tile: x chunk, row group, z layer
     const unsigned long long chunks = (total + kBatchChunk - 1) / kBatchChunk;
-    for (unsigned long long ch = blockIdx.x; ch < chunks; ch += gridDim.x)
+    for (unsigned long long ch = blockIdx.x; ch < chunks; ch += gridDim.x) {
+    bool fresh = true;
     for (unsigned long long w = ch * kBatchChunk; w < min(total, (ch + 1) * kBatchChunk); ++w) {
-        int lo = 0, hi = nlat - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (__ldg(&lat[mid].first) <= w) lo = mid;
-            else hi = mid - 1;
-        }
-        if (lo != cur_lat) {  // the same lattice for every thread of the block
+        if (w >= cur_end) {  // w and cur_end are the same for every thread of the block
+            int lo = 0, hi = nlat - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (__ldg(&lat[mid].first) <= w) lo = mid;
+                else hi = mid - 1;
+            }
             __syncthreads();
             const int* srcw = reinterpret_cast<const int*>(lat + lo);
             int* dstw = reinterpret_cast<int*>(&sl);
             for (int k = tid; k < (int)(sizeof(BatchLattice) / 4); k += 32 * ROWS) dstw[k] = __ldg(srcw + k);
             __syncthreads();
-            cur_lat = lo;
+            cur_end = lo + 1 < nlat ? __ldg(&lat[lo + 1].first) : total;
+            fresh = true;
+        }
+        if (fresh) {  // a lattice has fewer than 2^32 tiles
+            const unsigned local = (unsigned)(w - sl.first);
+            const unsigned t = local / (unsigned)sl.gx;
+            bx = (int)(local - t * (unsigned)sl.gx);
+            z = (int)(t / (unsigned)sl.gy);
+            ty = (int)(t - (unsigned)z * (unsigned)sl.gy);
+            fresh = false;
+        } else if (++bx == sl.gx) {
+            bx = 0;
+            if (++ty == sl.gy) {
+                ty = 0;
+                ++z;
+            }
         }
         const Geom& g = sl.g;
         const StepParams& p = sl.p;
@@ -677,11 +697,7 @@ __global__ void __launch_bounds__(32 * ROWS, 32 / ROWS) k_bulk_pairs_batch(const
         const PlanePtrs& pp = sl.pp[side];
         const T* __restrict__ fin = static_cast<const T*>(sl.pop[side]);
         T* __restrict__ fout = static_cast<T*>(const_cast<void*>(sl.pop[side ^ 1]));
-        const unsigned long long local = w - sl.first;
-        const int bx = (int)(local % (unsigned)sl.gx);
-        const unsigned long long t = local / (unsigned)sl.gx;
-        const int y = (int)(t % (unsigned)sl.gy) * ROWS + threadIdx.y;
-        const int z = (int)(t / (unsigned)sl.gy);
+        const int y = ty * ROWS + threadIdx.y;
         if (y >= g.ny) continue;
         const size_t row = (size_t)z * g.ny + y;
         const int k = 2 * threadIdx.x;
@@ -747,6 +763,7 @@ __global__ void __launch_bounds__(32 * ROWS, 32 / ROWS) k_bulk_pairs_batch(const
         const unsigned bad = collide_pair<Q, S>(v, p.tau, p.cs) & pair;
         if (bad) atomicOr(sl.diverged, 1);
         store_pair<Q, S>(pp, c, v, pair);
+    }
     }
 }
 

@@ -113,13 +113,13 @@ def polar_sweep(nx: int = 128, alphas=None, re: float = 5e3, u: float = 0.06, st
                 storage: str = "FP16_OFFSET", cs: float = 0.1, device: int = 0, tune: bool = True,
                 chunk: int = 50) -> PolarSweepResult:
     """Steps one lattice per angle as a batch and reduces the forces."""
-    from .batch import LbmBatch
+    from .batch import CANDIDATES, LbmBatch
     alphas = list(np.linspace(-4.0, 12.0, 9) if alphas is None else alphas)
     mem = make_members([dict(nx=nx, alpha=a, u=u, re=re) for a in alphas], storage, cs, device)
     solvers = [m[0] for m in mem]
     batch = LbmBatch(solvers)
     tuned = batch.Tune(4) if tune else None
-    done = 6 * (4 + 2) if tune else 0
+    done = len(CANDIDATES) * (4 + 2) if tune else 0
     avg_from = int(0.8 * steps)
     acc = np.zeros((len(alphas), 4))  # Fx, Fz, Fz * x_cp, count
     while done < steps:

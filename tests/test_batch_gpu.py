@@ -45,7 +45,7 @@ def test_batch_is_bit_identical_to_single_steps(gpu, storage, q):
     for s in single:
         s.Step(None, 17)
     _same(batched, single)
-    for rows, mult in ((4, 2), (16, 1)):
+    for rows, mult in ((4, 2), (16, 1), (0, 1)):
         b.Config(rows, mult)
         b.Step(4)
         for s in single:
@@ -60,15 +60,52 @@ def test_batch_is_bit_identical_to_single_steps(gpu, storage, q):
     b.close()
 
 
+def test_blocks_that_take_many_chunks(gpu):
+    """About 6M cells: with one wave of resident blocks every block takes
+    several chunks of tiles in turn, within a lattice and across lattice
+    ends (tile counts that are no multiple of the chunk), and the batch
+    still gives the bits of single stepping."""
+    from flowcraft_b200.batch import LbmBatch
+    from flowcraft_b200.lbm import LatticeModel, LbmSolver, Params, Storage, VoxelGrid
+    # tiles at 16 / 4 rows: 3668 / 13100, 612 / 2448, 3232 / 12120 (chunks of 8)
+    shapes = [((250, 100, 131), (80.0, 50.0, 65.0, 12.0)), ((130, 62, 51), (40.0, 31.0, 25.0, 6.0)),
+              ((200, 120, 101), (60.0, 60.0, 50.0, 10.0))]
+
+    def make():
+        out = []
+        for (nx, ny, nz), sph in shapes:
+            solid, sdf = geometry({"kind": "sphere", "dims": [nx, ny, nz], "center": list(sph[:3]), "r": sph[3]})
+            s = LbmSolver()
+            assert s.Init(0, VoxelGrid(nx, ny, nz, solid=solid.ravel(), signedDistance=sdf.ravel()),
+                          LatticeModel.D3Q19, Storage.FP16_OFFSET)
+            s.Reset(Params(tau=0.56, inletVelocity=0.06, smagorinskyCs=0.1), True)
+            out.append(s)
+        return out
+
+    batched, single = make(), make()
+    assert sum(s.CellCount() for s in batched) > 6_000_000
+    b = LbmBatch(batched)
+    for rows in (16, 4):
+        b.Config(rows, 1)
+        b.Step(4)
+        for s in single:
+            s.Step(None, 4)
+    _same(batched, single)
+    assert not any(s.HasDiverged() for s in batched)
+    b.close()
+    for s in batched + single:
+        s.close()
+
+
 def test_tuner_picks_a_shape_and_keeps_results(gpu):
     from flowcraft_b200.batch import LbmBatch
     batched, single = _make("FP16_OFFSET"), _make("FP16_OFFSET")
     b = LbmBatch(batched)
     r = b.Tune(steps=4)
-    assert (r["rows"], r["grid_mult"]) in [(4, 1), (4, 2), (8, 1), (8, 2), (16, 1), (16, 2)]
-    assert all(v > 0 for v in r["ms_per_step"].values())
+    assert (r["rows"], r["grid_mult"]) in [(4, 1), (4, 2), (8, 1), (8, 2), (16, 1), (16, 2), (0, 1)]
+    assert len(r["ms_per_step"]) == 7 and all(v > 0 for v in r["ms_per_step"].values())
     for s in single:
-        s.Step(None, 6 * (4 + 2))
+        s.Step(None, 7 * (4 + 2))
     b.Step(8)
     for s in single:
         s.Step(None, 8)
