@@ -59,7 +59,8 @@ CONFIGS = {
     "c3": dict(nx=0, ny=0, nz=0, geom="batch", u=0.0, re=0.0, lref=0.0, cs=0.1,
                desc="D3Q19 batch of 16 NACA 2412 wing lattices, sizes 64x32x32..256x128x128 (2:1:1) drawn with seed "
                     "20261203, chord 0.375 nx, AoA -8..14 deg, U 0.04-0.08, Re 1e3-2e4, FP16 offset, Smagorinsky "
-                    "Cs=0.1, one persistent launch per step over all lattices (autotuned block shape)"),
+                    "Cs=0.1, all lattices stepped as one batch per step in a CUDA graph (autotuned: one persistent "
+                    "launch, or the lattices' own bulk kernels side by side)"),
     # the precision-study lattice size: 384x192x192 NACA 0012 wing, chord 96, 4 deg
     "c2": dict(nx=384, ny=192, nz=192, geom="naca0012", u=0.06, re=1e4, lref=96.0, cs=0.1,
                desc="D3Q19 384x192x192 (14.2M cells), NACA 0012 wing chord 96 span 128 at 4 deg, U=0.06, "
