@@ -1521,11 +1521,19 @@ int batch_prepare(fc_lbm_batch* b, bool want_graph) {
     return FC_LBM_OK;
 }
 
+// Every call that steps the batch re-checks its members: a member may have
+// been shut down, re-initialized or given a learned closure since the batch
+// was created, and the batch kernels would then step it with the wrong
+// closure or layout instead of reproducing fc_lbm_step.
 int batch_check(fc_lbm_batch* b) {
-    for (fc_lbm* h : b->m)
-        if (!h->valid || h->device != b->device || h->q != b->q || h->storage != b->storage || h->closure_on ||
-            h->g.nx % 2 != 0)
-            return bfail(b, FC_LBM_ERR_INVALID_ARG, "a batch member changed (re-initialized, closure set or shut down)");
+    for (fc_lbm* h : b->m) {
+        if (!h->valid || h->device != b->device || h->q != b->q || h->storage != b->storage)
+            return bfail(b, FC_LBM_ERR_INVALID_ARG, "a batch member changed (shut down or re-initialized)");
+        if (h->closure_on)
+            return bfail(b, FC_LBM_ERR_UNSUPPORTED, "a batch member has a learned closure (set after batch create)");
+        if (in_place(h) || h->g.nx % 2 != 0)
+            return bfail(b, FC_LBM_ERR_UNSUPPORTED, "a batch member was re-initialized with AA streaming or odd nx");
+    }
     return FC_LBM_OK;
 }
 

@@ -622,16 +622,23 @@ cudaError_t launch_aero(int q, int storage, const void* f, const uint8_t* solid,
 // ---- statistics without allocation (fc_lbm_stats_noalloc) ----
 // The same k_stats / k_stats_final kernels as fc_lbm_readback_stats, with the
 // per-block partials in a fixed file-scope device array instead of memory the
-// solver allocated: one block per 2^17 cells, at most 4096 blocks, so the
-// array is 4096 * 12 doubles = 384 KiB and covers up to 2^29 cells. Each
-// launch writes every slot of the partials it uses before the final kernel
-// reads them, so nothing has to be cleared between calls.
+// solver allocated. The array holds 4096 blocks' partials (4096 * 12 doubles
+// = 384 KiB). The block count follows the allocating path's rule, one block
+// per 2048 cells, capped here by the array instead of at 148 * 16: the
+// reduction is grid-stride, so every cell is covered whatever the count, and
+// below the allocating path's cap (4.8M cells) both paths form the same
+// partial sums. Lattices are limited to 2^29 cells. Each launch writes every
+// slot of the partials it uses before the final kernel reads them, so nothing
+// has to be cleared between calls.
+//
+// The device address of the array is looked up once per device and cached for
+// the life of the process. A cudaDeviceReset destroys the module that holds
+// the array, so that cached address does not survive a reset; the header
+// documents this.
 namespace {
 
 constexpr int kNoAllocMaxBlocks = 4096;
-constexpr size_t kNoAllocCellsPerBlock = size_t(1) << 17;
-static_assert((unsigned long long)kNoAllocMaxBlocks * kNoAllocCellsPerBlock == FC_LBM_NOALLOC_MAX_CELLS,
-              "header limit must match the scratch size");
+constexpr size_t kNoAllocCellsPerBlock = size_t(1) << 11;  // kStatsThreads * 8, as stats_blocks()
 static_assert(fc::kStatsSlots == FC_LBM_STATS_SLOTS, "slot count must match the header");
 
 static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxBlocks * fc::kStatsSlots];
@@ -673,7 +680,8 @@ extern "C" FC_LBM_API int fc_lbm_stats_noalloc(const void* populations, const ui
     g.wpr = (nx + 31) / 32;
     g.nxy = (long long)nx * ny;
     g.n = n;
-    const int blocks = (int)((n + kNoAllocCellsPerBlock - 1) / kNoAllocCellsPerBlock);
+    const size_t want = (n + kNoAllocCellsPerBlock - 1) / kNoAllocCellsPerBlock;
+    const int blocks = (int)(want < 1 ? 1 : (want > (size_t)kNoAllocMaxBlocks ? (size_t)kNoAllocMaxBlocks : want));
     const int q = model == FC_LATTICE_D3Q19 ? 19 : 15;
     const cudaError_t e = fc::launch_stats(q, storage, populations, solid, signed_distance, g, scratch, blocks,
                                            out_slots, fc::kLayoutPlanes, static_cast<cudaStream_t>(stream));

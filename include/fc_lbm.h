@@ -439,7 +439,11 @@ FC_LBM_API int fc_lbm_batch_tune(fc_lbm_batch* b, int32_t steps, int32_t* rows, 
  *
  * All pointers are device memory on the calling thread's current device:
  * `populations` holds Q*N values in `storage`'s format (FC_STORAGE_*), laid
- * out f[i*N + cell] with N = nx*ny*nz; `solid` holds N bytes;
+ * out f[i*N + cell] with N = nx*ny*nz (plane-major, the layout of a ping-pong
+ * set and of fc_lbm_save_populations; a set streamed in place with
+ * FC_STREAMING_AA keeps population i of a cell in other slots between steps,
+ * and passing it here is a caller error that the call cannot detect: it reads
+ * the wrong slots); `solid` holds N bytes;
  * `signed_distance` holds N floats or is NULL. The result is written to the
  * device buffer `out_slots` (FC_LBM_STATS_SLOTS doubles: density sum, speed
  * sum, mass, Fx, Fy, Fz, fluid cell count, min density, max density, max
@@ -451,10 +455,12 @@ FC_LBM_API int fc_lbm_batch_tune(fc_lbm_batch* b, int32_t steps, int32_t* rows, 
  * process exits. It covers lattices up to FC_LBM_NOALLOC_MAX_CELLS cells;
  * larger ones are refused with FC_LBM_ERR_TOO_LARGE before any work is
  * queued. The first call on each device looks up that array's device address
- * once; make that first call before any stream capture begins. Every call
- * reuses the same array, so two calls whose work overlaps on the GPU (on
- * different streams without ordering) race; order them on one stream or with
- * events. */
+ * once and keeps it for the life of the process; make that first call before
+ * any stream capture begins. The kept address does not survive
+ * cudaDeviceReset (the reset unloads the array), so do not call this entry
+ * point on a device after resetting it. Every call reuses the same array, so
+ * two calls whose work overlaps on the GPU (on different streams without
+ * ordering) race; order them on one stream or with events. */
 #define FC_LBM_STATS_SLOTS 12
 #define FC_LBM_NOALLOC_MAX_CELLS 536870912ull
 #define FC_LBM_ERR_TOO_LARGE (-7)

@@ -60,11 +60,19 @@ class OracleStats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+def reference_tree() -> str:
+    """The FlowCraft source tree oracle/_ref is compiled from: $FLOWCRAFT_REF,
+    else the directory `reference` beside this repository's root."""
+    env = os.environ.get("FLOWCRAFT_REF")
+    return os.path.abspath(env) if env else os.path.abspath(os.path.join(HERE, "..", "..", "reference"))
+
+
 def build(force: bool = False) -> None:
     """Compile the oracle libraries (and oracle/_ref when the reference tree exists)."""
     need = force or not all(os.path.exists(_LIBS[k][0]) for k in ("f32", "f64"))
-    if need or (os.path.isdir("/root/reference") and not os.path.exists(_LIBS["ref"][0])):
-        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    ref = reference_tree()
+    if need or (os.path.isdir(ref) and not os.path.exists(_LIBS["ref"][0])):
+        subprocess.run(["make", "-s", "-C", HERE, f"REF={ref}"], check=True)
 
 
 def available(precision: str) -> bool:

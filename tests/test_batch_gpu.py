@@ -133,6 +133,26 @@ def test_batch_refuses_mismatched_members(gpu):
         LbmBatch([a[0], a[0]])
 
 
+def test_batch_refuses_member_given_a_closure_after_create(gpu):
+    """A learned closure set on a member after the batch was created is
+    refused at the next batch step instead of being stepped with Smagorinsky."""
+    from flowcraft_b200.batch import LbmBatch
+    from flowcraft_b200.closure import ClosureWeights
+    from flowcraft_b200.lbm import FC_LBM_ERR_UNSUPPORTED, LbmError
+    m = _make("FP16_OFFSET")
+    b = LbmBatch(m)
+    b.Step(2)
+    m[1].SetClosure(ClosureWeights.random(0))
+    with pytest.raises(LbmError) as ei:
+        b.Step(2)
+    assert ei.value.code == FC_LBM_ERR_UNSUPPORTED
+    with pytest.raises(LbmError):
+        b.Tune(1)
+    m[1].SetClosure(None)
+    b.Step(2)
+    b.close()
+
+
 def test_polar_sweep_small(gpu):
     """A 3-angle polar on 64x32x32 wings: finite forces, lift rising with
     angle, drag positive, the reference's polar fields filled in."""
