@@ -2,11 +2,13 @@
 """Benchmark of the B200 LBM time step (FlowCraft's LbmSolver::Step hot path).
 
 Workload (default, the large configuration the target is stated on): D3Q19,
-1024x512x512 = 268.4M cells, a procedural high-wing aircraft given as an SDF
-(ellipsoidal fuselage, tapered NACA 2412 wing, NACA 0012 tails), inlet
+1024x512x512 = 268.4M cells, a procedural high-wing aircraft mesh of 57,516
+triangles (ellipsoidal fuselage, tapered NACA 2412 wing, NACA 0012 tails)
+voxelized on the device by the library's voxelizer (fc_lbm_voxelize, solid
+mask and signed distance, so the Bouzidi links come from the mesh), inlet
 U = 0.05, Re = 1e5 on the 60-cell root chord (tau = 0.50009), Smagorinsky
-Cs = 0.1, free-slip side walls. Synthetic input: the geometry is built
-analytically on the device; there is no mesh file or dataset.
+Cs = 0.1, free-slip side walls. Synthetic input: the mesh is generated
+procedurally; there is no mesh file or dataset.
 
 One "step" is one full lattice update (every cell streamed, collided and
 written). ``value`` = whole-job GLUPS (cells x steps / s, solid cells
@@ -50,8 +52,9 @@ FALLBACK_HBM_GBS = 6650.0
 CONFIGS = {
     # the large configuration: 1024x512x512, aircraft, Re 1e5 on a 60-cell root chord
     "large": dict(nx=1024, ny=512, nz=512, geom="aircraft", u=0.05, re=1e5, lref=60.0, cs=0.1,
-                  desc="D3Q19 1024x512x512 (268.4M cells), procedural high-wing aircraft SDF, U=0.05, "
-                       "Re=1e5 on the 60-cell root chord (tau=0.50009), Smagorinsky Cs=0.1"),
+                  desc="D3Q19 1024x512x512 (268.4M cells), procedural high-wing aircraft mesh (57,516 triangles) "
+                       "voxelized on the device, U=0.05, Re=1e5 on the 60-cell root chord (tau=0.50009), "
+                       "Smagorinsky Cs=0.1"),
     # the plain-FP32 parity lattice: 128x64x64, sphere r=10, Re=100
     "c1": dict(nx=128, ny=64, nz=64, geom="sphere", u=0.05, re=100.0, lref=20.0, cs=0.1,
                desc="D3Q19 128x64x64 (524k cells), sphere r=10 at (40,32,32), U=0.05, Re=100 (tau=0.53), Cs=0.1"),
@@ -90,6 +93,11 @@ def parse_args(argv=None):
                     help="untimed steps from the seed before the warm-up of the learned variants (flow state)")
     ap.add_argument("--batch-shape", default=None,
                     help="c3 only: ROWSxMULT (e.g. 4x2, or 0x1 for per-member launches) instead of the autotuner")
+    ap.add_argument("--shard", action="store_true",
+                    help="one lattice split into z-slabs across the ranks (NCCL point-to-point halo exchange), "
+                         "FP16 offset storage with Smagorinsky; on one GPU, --shard-ranks slabs emulated with "
+                         "device copies as the exchange")
+    ap.add_argument("--shard-ranks", type=int, default=2, help="slabs emulated on one GPU with --shard at N=1")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -181,6 +189,54 @@ def ncu_traffic_per_cell(variant: str, developed: bool = False):
     return None
 
 
+def aircraft_on_device(cfg, device):
+    """The aircraft mesh voxelized on the device by the library: (solid u8,
+    sdf f32) torch tensors (nz, ny, nx) on `device` (a cuda device)."""
+    import torch
+
+    from flowcraft_b200 import meshes
+    from flowcraft_b200.voxelizer import VoxelizeOnGrid
+    nx, ny, nz = cfg["nx"], cfg["ny"], cfg["nz"]
+    pos, idx = meshes.aircraft_c5(nx)
+    g = VoxelizeOnGrid(pos, idx, (nx, ny, nz), 1.0, meshes.aircraft_c5_origin(nx, ny, nz),
+                       device=torch.device(device).index or 0)
+    return g.solid.view(nz, ny, nx), g.signedDistance.view(nz, ny, nx)
+
+
+def aircraft_on_host(cfg, z_lo, z_hi):
+    """Layers [z_lo, z_hi) of the same voxelization computed on the host by the
+    CPU restatement of the voxelizer (for the reference arm, which runs none
+    of the library's kernels). It voxelizes the aircraft's bounding box plus
+    a margin of 8 cells: a signed distance is finite only within a few cells
+    of a triangle, the cell centres are exact (whole-cell origin), and the
+    flood fill starts outside the aircraft, so that box classifies its cells
+    as the full lattice does, and every cell outside it is fluid with
+    distance +infinity."""
+    import numpy as np
+
+    from flowcraft_b200 import meshes
+    from oracle import oracle as orc
+    nx, ny, nz = cfg["nx"], cfg["ny"], cfg["nz"]
+    pos, idx = meshes.aircraft_c5(nx)
+    ox, oy, oz = meshes.aircraft_c5_origin(nx, ny, nz)
+    # lattice index ranges of the box: grid x spans world y, grid y world x
+    lo = [int(np.floor(pos[:, 1].min() - oy)) - 8, int(np.floor(pos[:, 0].min() - ox)) - 8,
+          int(np.floor(pos[:, 2].min() - oz)) - 8]
+    hi = [int(np.ceil(pos[:, 1].max() - oy)) + 8, int(np.ceil(pos[:, 0].max() - ox)) + 8,
+          int(np.ceil(pos[:, 2].max() - oz)) + 8]
+    lo = [max(0, v) for v in lo]
+    hi = [min(d, v) for d, v in zip((nx, ny, nz), hi)]
+    bs, bd = orc.voxelize(pos, idx, (hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]), 1.0,
+                          np.asarray((ox + lo[1], oy + lo[0], oz + lo[2]), np.float32))
+    solid = np.zeros((z_hi - z_lo, ny, nx), np.uint8)
+    sdf = np.full((z_hi - z_lo, ny, nx), np.inf, np.float32)
+    a, b = max(z_lo, lo[2]), min(z_hi, hi[2])
+    if a < b:
+        solid[a - z_lo:b - z_lo, lo[1]:hi[1], lo[0]:hi[0]] = bs[a - lo[2]:b - lo[2]]
+        sdf[a - z_lo:b - z_lo, lo[1]:hi[1], lo[0]:hi[0]] = bd[a - lo[2]:b - lo[2]]
+    return solid, sdf
+
+
 def build_geometry(cfg, device, z_lo=0, z_hi=None):
     """(solid u8, sdf f32) torch tensors (nz, ny, nx), or layers [z_lo, z_hi)."""
     import torch
@@ -188,7 +244,11 @@ def build_geometry(cfg, device, z_lo=0, z_hi=None):
     from flowcraft_b200 import geometry
     z_hi = cfg["nz"] if z_hi is None else z_hi
     if cfg["geom"] == "aircraft":
-        return geometry.aircraft_grid_torch(cfg["nx"], cfg["ny"], cfg["nz"], device=device, z_lo=z_lo, z_hi=z_hi)
+        if str(device).startswith("cuda"):
+            solid, sdf = aircraft_on_device(cfg, device)
+            return solid[z_lo:z_hi], sdf[z_lo:z_hi]
+        solid, sdf = aircraft_on_host(cfg, z_lo, z_hi)
+        return torch.from_numpy(solid), torch.from_numpy(sdf)
     if cfg["geom"] == "sphere":
         solid, sdf = geometry.sphere_grid(cfg["nx"], cfg["ny"], cfg["nz"], 40, 32, 32, 10)
         return (torch.from_numpy(solid[z_lo:z_hi].copy()).to(device),
@@ -476,10 +536,101 @@ def run_batch(args, cfg, rank, world, local_rank):
     return 0
 
 
+def run_shard(args, cfg, rank, world, local_rank):
+    """One lattice split into z-slabs (flowcraft_b200.shard): each rank steps
+    its slab and exchanges per step the 5 planes that stream across each cut
+    with its neighbours (NCCL point-to-point on the slab stream, overlapped
+    with the slab's interior layers). Events on the slab stream split a step
+    into the edge layers and their packing, the interior layers, the part
+    of the exchange the interior did not hide, and the unpacking. With one
+    process, --shard-ranks slabs are emulated on one GPU (device copies as
+    the exchange, no overlap)."""
+    import torch
+
+    from flowcraft_b200 import LatticeModel, Params, Storage, shard
+    dist_on = world > 1
+    torch.cuda.set_device(local_rank)
+    solid, sdf = build_geometry(cfg, f"cuda:{local_rank}")
+    params = Params(tau=tau_for(cfg), inletVelocity=cfg["u"], smagorinskyCs=cfg["cs"])
+    cells = cfg["nx"] * cfg["ny"] * cfg["nz"]
+    keys = ("edges_ms", "interior_ms", "exposed_exchange_ms", "unpack_ms")
+    split = dict.fromkeys(keys, 0.0)
+    if dist_on:
+        s, lay, st = shard.nccl_rank(solid, sdf, LatticeModel.D3Q19, Storage.FP16_OFFSET, params)
+        del solid, sdf
+        torch.cuda.empty_cache()
+        st.step(args.warmup)
+        barrier_sync(dist_on)
+        with st.on_stream():
+            start = torch.cuda.Event(enable_timing=True)
+            stop = torch.cuda.Event(enable_timing=True)
+            evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(args.steps)]
+            start.record()
+            for ev in evs:
+                ev[0].record()
+                st.edges()
+                h = st.ex.post(st.posts(st.dir_rows))
+                ev[1].record()
+                st.interior()
+                ev[2].record()
+                st.ex.wait(h)
+                ev[3].record()
+                st.finish()
+                ev[4].record()
+            stop.record()
+        stop.synchronize()
+        for ev in evs:
+            for k, key in enumerate(keys):
+                split[key] += ev[k].elapsed_time(ev[k + 1])
+        ms = start.elapsed_time(stop)
+        nranks, slabs = world, world
+        closers = [s]
+    else:
+        ranks = shard.emulated_ranks(solid, sdf, args.shard_ranks, local_rank, LatticeModel.D3Q19,
+                                     Storage.FP16_OFFSET, params)
+        del solid, sdf
+        torch.cuda.empty_cache()
+        steppers = [r[2] for r in ranks]
+        shard.step_emulated(steppers, args.warmup)
+        cmd = steppers[0].cmd
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record(cmd)
+        shard.step_emulated(steppers, args.steps)
+        stop.record(cmd)
+        stop.synchronize()
+        ms = start.elapsed_time(stop)
+        split = None
+        nranks, slabs = 1, args.shard_ranks
+        closers = [r[0] for r in ranks]
+    ms = allreduce_max(ms, dist_on)
+    if split is not None:
+        split = {k: allreduce_max(v, dist_on) / args.steps for k, v in split.items()}
+    for s in closers:
+        s.close()
+    if rank != 0:
+        return 0
+    halo = shard.DIR_PLANES * cfg["nx"] * cfg["ny"] * 2
+    line = {"metric": METRIC, "value": cells * args.steps / (ms / 1e3) / 1e9, "unit": "GLUPS", "n_gpus": nranks,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: procedural aircraft mesh voxelized on the device, no dataset",
+            "config": {"workload": cfg["desc"], "lattice": "D3Q19", "storage": "fp16_offset", "closure": "Smagorinsky",
+                       "parallelism": (f"z-slabs x{world}, NCCL point-to-point halo exchange" if dist_on else
+                                       f"{slabs} z-slabs emulated on one GPU, device copies as the exchange"),
+                       "halo_bytes_per_side_per_step": halo},
+            "step_split_ms": split, "gpu_launches": None}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ours(args, cfg, rank, world, local_rank):
     import torch
     if cfg["geom"] == "batch":
         return run_batch(args, cfg, rank, world, local_rank)
+    if args.shard:
+        return run_shard(args, cfg, rank, world, local_rank)
     dist_on = world > 1
     torch.cuda.set_device(local_rank)
     dev_index = local_rank
@@ -523,18 +674,22 @@ def run_ours(args, cfg, rank, world, local_rank):
         return 0
     variants_out = {}
     for v, r in results.items():
+        # compact, so that every variant fits in a short tail of the output
         variants_out[v] = {
-            "glups": world * cells * args.steps / (r["total_ms"] / 1e3) / 1e9, "ms_per_step": r["ms_per_step"],
-            "bulk_ms_per_launch": r["bulk_ms_per_launch"], "boundary_ms_per_launch": r["boundary_ms_per_launch"],
-            "bulk_gbs": r["bulk_gbs"], "roofline_frac": r["bulk_gbs"] / peak if r["bulk_gbs"] else None,
-            "bytes_per_cell_update": r["bytes_per_cell"], "clocks": r["clocks"], "stats_after": r["stats_after"],
-            "closure_coverage": r["closure_coverage"], "spinup_steps": r["spinup_steps"],
+            "glups": round(world * cells * args.steps / (r["total_ms"] / 1e3) / 1e9, 2),
+            "ms": round(r["ms_per_step"], 3), "bulk_ms": round(r["bulk_ms_per_launch"], 3),
+            "frac": round(r["bulk_gbs"] / peak, 3) if r["bulk_gbs"] else None, "B_cell": r["bytes_per_cell"],
+            "mhz": r["clocks"]["sm_mhz"] if r["clocks"] else None,
         }
+        if r["closure_coverage"]:
+            variants_out[v]["mlp_warps"] = round(r["closure_coverage"]["warp_fraction"], 4)
+        if r["stats_after"]["has_nan"]:
+            variants_out[v]["nan"] = True
     line = {
         "metric": METRIC, "value": value, "unit": "GLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic: analytic procedural geometry built on the device, no dataset",
+        "data": "synthetic: procedural aircraft mesh voxelized on the device, no dataset",
         "config": {"workload": cfg["desc"], "lattice": "D3Q19", "nx": cfg["nx"], "ny": cfg["ny"], "nz": cfg["nz"],
                    "cells": cells, "storage": head["variant"], "collision": "regularized, FP32",
                    "closure": ("learned MLP 5-32-32-1 (BF16 tensor-core MMA, FP32 accumulate) per cell, Smagorinsky "
@@ -545,7 +700,8 @@ def run_ours(args, cfg, rank, world, local_rank):
                                   if head["spinup_steps"] else f"timed after {args.warmup} steps from the seed"),
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "no flush: the population set (10.2 GB fp16 / 20.4 GB fp32 per copy) exceeds the 126 MB L2",
-                   "boundary_cells": head["boundary_cells"], "bouzidi_links": head["bouzidi_links"]},
+                   "boundary_cells": head["boundary_cells"], "bouzidi_links": head["bouzidi_links"],
+                   "closure_coverage": head["closure_coverage"]},
         "variants": variants_out,
         "roofline": roofline,
         "cpu_baseline": cpu,

@@ -4,7 +4,10 @@
 (``fc_lbm_set_closure`` in include/fc_lbm.h): 5 inputs -> 32 -> 32 -> 1 with
 ReLU, inputs normalized by ``mean`` / ``std``, output nu_t = relu(z) *
 ``out_scale``, and the training range [lo, hi] of inputs 0-2 outside which a
-cell keeps the Smagorinsky closure. The inputs are
+cell keeps the Smagorinsky closure. ``wall_min`` (cells) extends that
+fallback to the cells nearer a wall, and ``trust`` > 0 anchors the network to
+Smagorinsky: 3 nu_t stays within a factor ``trust`` of the Smagorinsky
+value. The inputs are
   0 log2(|Pi_neq| / rho), 1 tr(Pi_neq) / |Pi_neq|, 2 det(Pi_neq) / |Pi_neq|^3,
   3 wall distance (cells), 4 filter width.
 Weights are input-major (w1[k, j] feeds input k to hidden unit j).
@@ -34,6 +37,10 @@ class ClosureWeights:
     lo: np.ndarray = field(default_factory=lambda: np.full(3, -np.inf, np.float32))
     hi: np.ndarray = field(default_factory=lambda: np.full(3, np.inf, np.float32))
     filter_width: float = 1.0
+    # cells nearer a wall than wall_min cells keep Smagorinsky; trust > 0 holds
+    # 3 nu_t within [d / trust, d * trust] of Smagorinsky's d (0: off)
+    wall_min: float = 0.0
+    trust: float = 0.0
     meta: dict = field(default_factory=dict)
 
     @staticmethod

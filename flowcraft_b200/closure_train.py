@@ -127,12 +127,39 @@ def smagorinsky_nu(x0, tau_c: float, cs: float):
     return (te - tau_c) / 3.0
 
 
+def perturb_start(s, u: float, seed: int, amplitude: float = 0.1):
+    """Replaces a solver's mid-speed start by the same field plus a smooth
+    seeded transverse perturbation (ResetFromField): a few sine modes of
+    amplitude `amplitude` * u across y and z, with seeded wavenumbers and
+    phases, so that runs of the same geometry and Reynolds number develop
+    different wakes."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = s.Nx(), s.Ny(), s.Nz()
+    f = s.ReadbackField().reshape(nz, ny, nx, 4).copy()
+    z = (np.arange(nz) + 0.5)[:, None, None] / nz
+    y = (np.arange(ny) + 0.5)[None, :, None] / ny
+    x = (np.arange(nx) + 0.5)[None, None, :] / nx
+    du = np.zeros((3, nz, ny, nx), np.float64)
+    for comp in (1, 2):
+        for _ in range(3):
+            kx, ky, kz = rng.integers(1, 4, size=3)
+            ph = rng.uniform(0, 2 * np.pi, size=3)
+            du[comp] += (np.sin(2 * np.pi * kx * x + ph[0]) * np.sin(2 * np.pi * ky * y + ph[1]) *
+                         np.sin(2 * np.pi * kz * z + ph[2]))
+    du *= amplitude * u / 3.0
+    fluid = ~s.SolidMask().reshape(nz, ny, nx).astype(bool)
+    for comp in range(3):
+        f[..., 1 + comp] += np.where(fluid, du[comp], 0.0).astype(np.float32)
+    s.ResetFromField(f.ravel())
+
+
 def collect_samples(cases, device: int = 0, filter_width: float = 2.0):
     """Runs each fine case and gathers closure samples at its checkpoints.
 
     `cases`: iterable of dicts with keys solid, sdf (numpy (nz, ny, nx)), params
-    (flowcraft_b200.lbm.Params), warmup, every, count. Returns (samples tensor,
-    list of the coarse molecular tau of each case's rows)."""
+    (flowcraft_b200.lbm.Params), warmup, every, count, and optionally seed: a
+    seeded perturbation of the mid-speed start (perturb_start). Returns
+    (samples tensor, list of the coarse molecular tau of each case's rows)."""
     import torch
 
     from .lbm import LatticeModel, LbmSolver, Storage, VoxelGrid
@@ -145,6 +172,8 @@ def collect_samples(cases, device: int = 0, filter_width: float = 2.0):
         if not s.Init(device, g, LatticeModel.D3Q19, Storage.FP32):
             raise RuntimeError(s.LastError())
         s.Reset(case["params"], True)
+        if case.get("seed") is not None:
+            perturb_start(s, case["params"].inletVelocity, case["seed"])
         s.Step(None, case["warmup"])
         for _ in range(case["count"]):
             s.Step(None, case["every"])
@@ -214,10 +243,15 @@ def train_closure(samples, tau_c, device: int = 0, epochs: int = 20, batch: int 
     return cw, rep
 
 
+C4_REYNOLDS = (5e3, 1.6e4, 5e4)  # one per seed, log-spaced over Re 5e3 .. 5e4
+
+
 def c4_cases(scale: int = 1):
     """The training set of the closure: fine lattices of 512x256x256 (divided
-    by `scale` per axis) around a sphere and a NACA 2412 wing at three
-    Reynolds numbers, Smagorinsky Cs 0.1, sampled at three instants each."""
+    by `scale` per axis) around a sphere and a NACA 2412 wing (6 deg), three
+    seeds each: seed k runs at Reynolds number C4_REYNOLDS[k] from a
+    mid-speed start with seed k's perturbation (perturb_start); Smagorinsky
+    Cs 0.1, sampled at three instants each."""
     from . import geometry
     from .lbm import Params
     nx, ny, nz = 512 // scale, 256 // scale, 256 // scale
@@ -226,11 +260,13 @@ def c4_cases(scale: int = 1):
     sphere = geometry.sphere_grid(nx, ny, nz, nx * 0.3, ny * 0.5, nz * 0.5, nz * 0.09)
     chord = 0.375 * nx / 2
     wing = geometry.naca_wing_grid(nx, ny, nz, chord=chord, span=ny * 0.6, aoa_deg=6, digits="2412")
-    for (solid, sdf), lref, re in ((sphere, 2 * nz * 0.09, 5e3), (wing, chord, 2e4), (sphere, 2 * nz * 0.09, 5e4)):
-        nu = u * lref / re
-        cases.append(dict(solid=np.asarray(solid), sdf=np.asarray(sdf).ravel(),
-                          params=Params(tau=0.5 + 3 * nu, inletVelocity=u, smagorinskyCs=0.1),
-                          warmup=3 * nx, every=nx // 2, count=3))
+    for geo, (solid, sdf), lref in (("sphere", sphere, 2 * nz * 0.09), ("wing2412", wing, chord)):
+        for seed, re in enumerate(C4_REYNOLDS):
+            nu = u * lref / re
+            cases.append(dict(name=f"{geo}_re{re:.0e}_seed{seed}", solid=np.asarray(solid),
+                              sdf=np.asarray(sdf).ravel(),
+                              params=Params(tau=0.5 + 3 * nu, inletVelocity=u, smagorinskyCs=0.1),
+                              warmup=3 * nx, every=nx // 2, count=3, seed=seed))
     return cases
 
 

@@ -158,13 +158,27 @@ cudaError_t launch_wall_distance(const uint8_t* solid, const Geom& g, uint8_t* o
 // ---- training samples: a 2x box filter of a fine lattice ----
 //
 // Coarse cell X covers the fine cells 2X + {0,1}^3. From the fine
-// populations it gets the box-filtered density, momentum and momentum flux:
+// populations it gets the box-filtered density, momentum, momentum flux and
+// viscous stress:
 //   rho = <rho_f>, u = <rho_f u_f> / rho,
-//   tau_sgs = <rho_f u_f u_f> - rho u u          (the sub-grid stress),
-// and, with S the strain of the filtered velocity by central differences
-// over the coarse neighbours, the target eddy viscosity is the least-squares
-// fit of tau_sgs_dev = -2 rho nu S_dev:
-//   nu* = max(0, -tau_sgs_dev : S_dev / (2 rho S_dev : S_dev)).
+//   tau_sgs = <rho_f u_f u_f> - rho u u          (the resolved sub-grid stress),
+//   V = <V_f>                                    (the fine cells' viscous stress).
+// V_f is the whole viscous stress a fine cell carries, molecular and its own
+// Smagorinsky eddy viscosity: its stored populations are post-collision, so
+// their non-equilibrium stress is Pi* = (1 - 1/tau_f') Pi_neq with the cell's
+// tau_f' = (tau_f + sqrt(tau_f^2 + k |Pi_neq| / rho)) / 2, k = 18 sqrt2 Cs^2
+// (the step's Smagorinsky). Eliminating Pi_neq gives
+//   (tau_f' - tau_f) (1 - tau_f') = k |Pi*| / (4 rho),
+// a quadratic whose root next to tau_f is tau_f', and then
+//   V_f = 2 rho c_s^2 (tau_f' - 1/2) S_f = (tau_f' - 1/2) / (1 - tau_f') Pi*.
+// The filtered flow's momentum balance carries the stress V - tau_sgs, so
+// with S the strain of the filtered velocity by central differences over
+// the coarse neighbours, the coarse cell's total viscosity is the
+// least-squares fit of (V - tau_sgs)_dev = 2 rho nu S_dev, and the target
+// eddy viscosity is that minus the coarse molecular viscosity:
+//   nu* = max(0, (V - tau_sgs)_dev : S_dev / (2 rho S_dev : S_dev) - (tau_c - 1/2) / 3).
+// (Viscosity and strain are in each lattice's own units; their product, a
+// stress, is the same number on both.)
 // The inputs are those a coarse cell relaxing with tau_c + 3 nu* sees: the
 // regularized scheme's non-equilibrium stress is Pi = -2 rho c_s^2 tau_eff S
 // (Chapman-Enskog), so the samples carry the invariants of
@@ -173,7 +187,7 @@ cudaError_t launch_wall_distance(const uint8_t* solid, const Geom& g, uint8_t* o
 // (dx and dt both double), strains and viscosities are in coarse units.
 namespace {
 
-constexpr int kCoarseFields = 10;  // rho, u (3), tau_sgs (6)
+constexpr int kCoarseFields = 16;  // rho, u (3), tau_sgs (6), V (6)
 constexpr int kWaitTimeoutMs = 600000;
 
 // Waits for `s` by polling an event with a growing sleep, so a stuck device
@@ -206,7 +220,8 @@ cudaError_t wait_bounded(cudaStream_t s, bool* timed_out) {
 
 template <int Q, class S>
 __global__ void k_coarse_fields(const typename S::T* __restrict__ f, const uint8_t* __restrict__ solid, Geom fg,
-                                Geom cg, uint8_t* __restrict__ csolid, float* __restrict__ cf) {
+                                Geom cg, float tau_f, float cs_f, uint8_t* __restrict__ csolid,
+                                float* __restrict__ cf) {
     using L = Lattice<Q>;
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < cg.n; c += (size_t)gridDim.x * blockDim.x) {
         const int zc = (int)(c / (size_t)cg.nxy);
@@ -214,7 +229,7 @@ __global__ void k_coarse_fields(const typename S::T* __restrict__ f, const uint8
         const int yc = (int)(rem / cg.nx);
         const int xc = (int)(rem - (size_t)yc * cg.nx);
         bool any_solid = false;
-        double rs = 0, mx = 0, my = 0, mz = 0, uu[6] = {0, 0, 0, 0, 0, 0};
+        double rs = 0, mx = 0, my = 0, mz = 0, uu[6] = {0, 0, 0, 0, 0, 0}, vs[6] = {0, 0, 0, 0, 0, 0};
         for (int k = 0; k < 8; ++k) {
             const size_t fc = ((size_t)(2 * zc + (k >> 2)) * fg.ny + (2 * yc + ((k >> 1) & 1))) * fg.nx +
                               (2 * xc + (k & 1));
@@ -223,15 +238,31 @@ __global__ void k_coarse_fields(const typename S::T* __restrict__ f, const uint8
                 continue;
             }
             float rho = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
+            double m2[6] = {0, 0, 0, 0, 0, 0};  // sum f e_a e_b: xx yy zz xy xz yz
             static_for<0, Q>([&](auto I) {
                 constexpr int i = decltype(I)::value;
+                constexpr int X = L::ex(i), Y = L::ey(i), Z = L::ez(i);
                 const float v = load_pop_c<Q, S, i>(f, fg.n, fc);
                 rho += v;
-                if constexpr (L::ex(i) != 0) jx += (float)L::ex(i) * v;
-                if constexpr (L::ey(i) != 0) jy += (float)L::ey(i) * v;
-                if constexpr (L::ez(i) != 0) jz += (float)L::ez(i) * v;
+                if constexpr (X != 0) jx += (float)X * v;
+                if constexpr (Y != 0) jy += (float)Y * v;
+                if constexpr (Z != 0) jz += (float)Z * v;
+                m2[0] += (double)(X * X) * v, m2[1] += (double)(Y * Y) * v, m2[2] += (double)(Z * Z) * v;
+                m2[3] += (double)(X * Y) * v, m2[4] += (double)(X * Z) * v, m2[5] += (double)(Y * Z) * v;
             });
             const double ux = jx / rho, uy = jy / rho, uz = jz / rho;
+            // the cell's post-collision non-equilibrium stress, its relaxation
+            // time and its viscous stress (see above)
+            const double pr = (double)rho / 3.0;
+            const double pst[6] = {m2[0] - pr - rho * ux * ux, m2[1] - pr - rho * uy * uy, m2[2] - pr - rho * uz * uz,
+                                   m2[3] - rho * ux * uy, m2[4] - rho * ux * uz, m2[5] - rho * uy * uz};
+            const double pmag = sqrt(pst[0] * pst[0] + pst[1] * pst[1] + pst[2] * pst[2] +
+                                     2.0 * (pst[3] * pst[3] + pst[4] * pst[4] + pst[5] * pst[5]));
+            const double kq = 18.0 * 1.41421356 * (double)cs_f * (double)cs_f;
+            const double disc = (1.0 - tau_f) * (1.0 - tau_f) - kq * pmag / (rho > 1e-6f ? (double)rho : 1e-6);
+            const double te = 0.5 * ((1.0 + tau_f) - sqrt(disc > 0.0 ? disc : 0.0));
+            const double vf = (te - 0.5) / (1.0 - te);
+            for (int k = 0; k < 6; ++k) vs[k] += vf * pst[k];
             rs += rho;
             mx += jx, my += jy, mz += jz;
             uu[0] += rho * ux * ux, uu[1] += rho * uy * uy, uu[2] += rho * uz * uz;
@@ -248,6 +279,7 @@ __global__ void k_coarse_fields(const typename S::T* __restrict__ f, const uint8
         o[4] = (float)(uu[0] / 8.0 - rho * ux * ux), o[5] = (float)(uu[1] / 8.0 - rho * uy * uy);
         o[6] = (float)(uu[2] / 8.0 - rho * uz * uz), o[7] = (float)(uu[3] / 8.0 - rho * ux * uy);
         o[8] = (float)(uu[4] / 8.0 - rho * ux * uz), o[9] = (float)(uu[5] / 8.0 - rho * uy * uz);
+        for (int k = 0; k < 6; ++k) o[10 + k] = (float)(vs[k] / 8.0);
     }
 }
 
@@ -282,7 +314,8 @@ __device__ SampleOut coarse_sample(const uint8_t* __restrict__ csolid, const flo
         for (int b = 0; b < 3; ++b) sd[a][b] = sm[a][b] - (a == b ? tr : 0.0);
     const float* o = cf + c * kCoarseFields;
     const double rho = o[0];
-    const double t6[6] = {o[4], o[5], o[6], o[7], o[8], o[9]};
+    // the stress the coarse cell's viscosity must carry: V - tau_sgs
+    const double t6[6] = {o[10] - o[4], o[11] - o[5], o[12] - o[6], o[13] - o[7], o[14] - o[8], o[15] - o[9]};
     const double ttr = (t6[0] + t6[1] + t6[2]) / 3.0;
     const double td[3][3] = {{t6[0] - ttr, t6[3], t6[4]}, {t6[3], t6[1] - ttr, t6[5]}, {t6[4], t6[5], t6[2] - ttr}};
     double tds = 0.0, sds = 0.0;
@@ -292,7 +325,7 @@ __device__ SampleOut coarse_sample(const uint8_t* __restrict__ csolid, const flo
             sds += sd[a][b] * sd[a][b];
         }
     if (!(sds > 1e-18) || !(rho > 0.0)) return r;
-    double nu = -tds / (2.0 * rho * sds);
+    double nu = tds / (2.0 * rho * sds) - ((double)tau_c - 0.5) / 3.0;
     nu = nu > 0.0 ? nu : 0.0;
     // the stress a coarse cell relaxing with tau_c + 3 nu carries
     const double k = -(2.0 / 3.0) * rho * ((double)tau_c + 3.0 * nu);
@@ -336,31 +369,31 @@ __global__ void k_sample_write(const uint8_t* __restrict__ csolid, const float* 
 }
 
 template <int Q, class S>
-cudaError_t coarse_fields_t(const void* f, const uint8_t* solid, const Geom& fg, const Geom& cg, uint8_t* csolid,
-                            float* cf, cudaStream_t s) {
+cudaError_t coarse_fields_t(const void* f, const uint8_t* solid, const Geom& fg, const Geom& cg, float tau_f,
+                            float cs_f, uint8_t* csolid, float* cf, cudaStream_t s) {
     const int blocks = (int)((cg.n + 255) / 256 < 148 * 16 ? (cg.n + 255) / 256 : 148 * 16);
-    k_coarse_fields<Q, S><<<blocks, 256, 0, s>>>((const typename S::T*)f, solid, fg, cg, csolid, cf);
+    k_coarse_fields<Q, S><<<blocks, 256, 0, s>>>((const typename S::T*)f, solid, fg, cg, tau_f, cs_f, csolid, cf);
     return cudaGetLastError();
 }
 
 cudaError_t coarse_fields(int q, int storage, const void* f, const uint8_t* solid, const Geom& fg, const Geom& cg,
-                          uint8_t* csolid, float* cf, cudaStream_t s) {
+                          float tau_f, float cs_f, uint8_t* csolid, float* cf, cudaStream_t s) {
     if (q == 19) {
-        if (storage == 0) return coarse_fields_t<19, StoreF32>(f, solid, fg, cg, csolid, cf, s);
-        if (storage == 1) return coarse_fields_t<19, StoreF16>(f, solid, fg, cg, csolid, cf, s);
-        if (storage == 2) return coarse_fields_t<19, StoreBF16>(f, solid, fg, cg, csolid, cf, s);
+        if (storage == 0) return coarse_fields_t<19, StoreF32>(f, solid, fg, cg, tau_f, cs_f, csolid, cf, s);
+        if (storage == 1) return coarse_fields_t<19, StoreF16>(f, solid, fg, cg, tau_f, cs_f, csolid, cf, s);
+        if (storage == 2) return coarse_fields_t<19, StoreBF16>(f, solid, fg, cg, tau_f, cs_f, csolid, cf, s);
     } else if (q == 15) {
-        if (storage == 0) return coarse_fields_t<15, StoreF32>(f, solid, fg, cg, csolid, cf, s);
-        if (storage == 1) return coarse_fields_t<15, StoreF16>(f, solid, fg, cg, csolid, cf, s);
-        if (storage == 2) return coarse_fields_t<15, StoreBF16>(f, solid, fg, cg, csolid, cf, s);
+        if (storage == 0) return coarse_fields_t<15, StoreF32>(f, solid, fg, cg, tau_f, cs_f, csolid, cf, s);
+        if (storage == 1) return coarse_fields_t<15, StoreF16>(f, solid, fg, cg, tau_f, cs_f, csolid, cf, s);
+        if (storage == 2) return coarse_fields_t<15, StoreBF16>(f, solid, fg, cg, tau_f, cs_f, csolid, cf, s);
     }
     return cudaErrorInvalidValue;
 }
 
 }  // namespace
 
-int closure_samples(int q, int storage, const void* f, const uint8_t* solid, const Geom& fg, float tau_c,
-                    float filter_width, float* out, int64_t capacity, int64_t* count, cudaStream_t s) {
+int closure_samples(int q, int storage, const void* f, const uint8_t* solid, const Geom& fg, float tau_f, float cs_f,
+                    float tau_c, float filter_width, float* out, int64_t capacity, int64_t* count, cudaStream_t s) {
     Geom cg{};
     cg.nx = fg.nx / 2, cg.ny = fg.ny / 2, cg.nz = fg.nz / 2;
     cg.wpr = (cg.nx + 31) / 32;
@@ -386,7 +419,7 @@ int closure_samples(int q, int storage, const void* f, const uint8_t* solid, con
         ok(cudaMallocAsync(&tmp, cg.n, s)) && ok(cudaMallocAsync(&cf, cg.n * kCoarseFields * sizeof(float), s)) &&
         ok(cudaMallocAsync(&flags, cg.n * sizeof(uint32_t), s)) &&
         ok(cudaMallocAsync(&pos, (cg.n + 1) * sizeof(uint32_t), s)) &&
-        ok(coarse_fields(q, storage, f, solid, fg, cg, csolid, cf, s)) &&
+        ok(coarse_fields(q, storage, f, solid, fg, cg, tau_f, cs_f, csolid, cf, s)) &&
         ok(launch_wall_distance(csolid, cg, cwall, tmp, s))) {
         k_sample_flags<<<blocks, 256, 0, s>>>(csolid, cf, cwall, cg, tau_c, filter_width, flags);
         if (ok(cudaGetLastError()) && ok(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, flags, pos, (int64_t)cg.n, s)) &&

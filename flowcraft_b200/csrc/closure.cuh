@@ -118,6 +118,26 @@ __device__ __forceinline__ bool closure_in_range(const ClosureDev& cl, float x0,
     return closure_x0_in_range(cl, x0) && closure_x12_in_range(cl, x1, x2);
 }
 
+// The near-wall fallback: a cell whose wall-distance byte (1/16 cells) is
+// below cl.wall_min keeps the Smagorinsky closure.
+__device__ __forceinline__ bool closure_wall_ok(const ClosureDev& cl, unsigned wd) { return wd >= cl.wall_min; }
+
+// True when the learned nu_t is held inside a band around the Smagorinsky
+// value, so every covered cell also needs that value (smagorinsky_d3).
+__device__ __forceinline__ bool closure_anchored(const ClosureDev& cl) { return cl.trust > 0.0f; }
+
+// Relaxation factor g = (1 - 1/tau_eff) * 4.5 of a cell the MLP covers.
+// Unanchored: tau_eff = tau + 3 nu. Anchored (trust factor k > 0): 3 nu is
+// clamped into [ds / k, ds k], ds = 3 nu of the Smagorinsky closure, so the
+// Smagorinsky value bounds how far the network may move the cell.
+__device__ __forceinline__ float closure_g(const ClosureDev& cl, float nu, float tau, float ds) {
+    if (cl.trust > 0.0f) {
+        const float d = fminf(fmaxf(3.0f * nu, ds * cl.inv_trust), ds * cl.trust);
+        return (1.0f - __fdividef(1.0f, tau + d)) * 4.5f;
+    }
+    return (1.0f - __fdividef(1.0f, fmaf(3.0f, nu, tau))) * 4.5f;
+}
+
 // Packs a cell's five normalized inputs and the constant 1 that carries the
 // first layer's bias into the three BF16 pairs an A fragment row of K = 8
 // holds per lane quarter: (x0,x1) (x2,x3) (x4,1).

@@ -133,6 +133,15 @@ __device__ __forceinline__ float smagorinsky_g(float pp, float rho, float inv, f
     return (1.0f - __fdividef(2.0f, tau + t2 * rsqrtf(t2))) * 4.5f;
 }
 
+// 3 nu_t = tau_eff - tau of one cell under the Smagorinsky closure, from the
+// same operations as smagorinsky_g (the learned closure's anchor).
+__device__ __forceinline__ float smagorinsky_d3(float pp, float rho, float inv, float tau, float cs) {
+    const float k0 = (18.0f * 1.41421356f) * cs * cs;
+    const float pim = pp > 0.0f ? pp * rsqrtf(pp) : 0.0f;
+    const float t2 = fmaf(k0, pim * (rho < 1e-6f ? 1e6f : inv), tau * tau);
+    return fmaf(0.5f, tau + t2 * rsqrtf(t2), -tau);
+}
+
 // Second half: post-collision offsets of both cells from their moments and
 // relaxation factors g.
 template <int Q>

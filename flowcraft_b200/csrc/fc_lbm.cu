@@ -810,13 +810,17 @@ int fc_lbm_set_closure(fc_lbm* h, const fc_closure* c) {
               std::isfinite(c->filter_width);
     for (int k = 0; k < FC_CLOSURE_INPUTS; ++k) ok = ok && std::isfinite(c->mean[k]) && c->std[k] > 0.0f;
     for (int k = 0; k < 3; ++k) ok = ok && !(c->lo[k] > c->hi[k]);
+    ok = ok && std::isfinite(c->min_wall_distance) && c->min_wall_distance >= 0.0f && std::isfinite(c->trust_factor) &&
+         (c->trust_factor == 0.0f || c->trust_factor >= 1.0f);
     const int H = FC_CLOSURE_HIDDEN;
     for (int i = 0; i < FC_CLOSURE_INPUTS * H && ok; ++i) ok = std::isfinite(c->w1[i]);
     for (int i = 0; i < H * H && ok; ++i) ok = std::isfinite(c->w2[i]);
     for (int i = 0; i < H && ok; ++i)
         ok = std::isfinite(c->b1[i]) && std::isfinite(c->b2[i]) && std::isfinite(c->w3[i]);
     if (!ok)
-        return fail(h, FC_LBM_ERR_INVALID_ARG, "closure parameters must be finite, with std > 0 and out_scale > 0");
+        return fail(h, FC_LBM_ERR_INVALID_ARG,
+                    "closure parameters must be finite, with std > 0, out_scale > 0, min_wall_distance >= 0 and "
+                    "trust_factor 0 or >= 1");
     DeviceGuard dg(h->device);
     if (!h->d_wall) {
         uint8_t* tmp = nullptr;
@@ -857,6 +861,11 @@ int fc_lbm_set_closure(fc_lbm* h, const fc_closure* c) {
         cd.hi[k] = c->hi[k];
     }
     cd.filter_width = c->filter_width;
+    // the wall-distance bytes count 1/16 cells; a cell keeps Smagorinsky below this byte
+    const float wm = std::ceil(c->min_wall_distance * 16.0f);
+    cd.wall_min = wm > 255.0f ? 256u : (unsigned)wm;
+    cd.trust = c->trust_factor;
+    cd.inv_trust = c->trust_factor > 0.0f ? 1.0f / c->trust_factor : 0.0f;
     h->closure = cd;
     h->closure_on = true;
     return FC_LBM_OK;
@@ -870,8 +879,8 @@ int fc_lbm_closure_samples(fc_lbm* h, float filter_width, float* out, int64_t ca
     FC_RC(wait_stream(h, kTransferTimeoutMs));  // every queued step first
     // the molecular relaxation time of the 2x coarser lattice (nu halves)
     const float tau_c = 0.5f + 0.5f * (h->params.tau - 0.5f);
-    const int rc = fc::closure_samples(h->q, h->storage, h->pop[h->cur], h->d_solid, h->g, tau_c, filter_width, out,
-                                       capacity, count, h->stream);
+    const int rc = fc::closure_samples(h->q, h->storage, h->pop[h->cur], h->d_solid, h->g, h->params.tau,
+                                       h->params.smagorinsky_cs, tau_c, filter_width, out, capacity, count, h->stream);
     h->launches += 5;
     if (rc != FC_LBM_OK && rc != FC_LBM_ERR_TOO_LARGE) return fail(h, rc, "closure samples failed");
     return rc;
@@ -958,6 +967,37 @@ int fc_lbm_layer_copy(fc_lbm* h, int32_t z, int32_t next, void* buffer, int32_t 
                                     : cudaMemcpy2DAsync(pop, pitch, buffer, width, width, (size_t)h->q,
                                                         cudaMemcpyDeviceToDevice, s);
     FC_TRY(h, e, "layer copy");
+    return leave_stream(h, s);
+}
+
+int fc_lbm_layer_copy_dir(fc_lbm* h, int32_t z, int32_t next, void* buffer, int32_t to_buffer, int32_t ez,
+                          void* stream) {
+    if (ez == 0) return fc_lbm_layer_copy(h, z, next, buffer, to_buffer, stream);
+    FC_RC(check_ready(h));
+    if (!buffer || z < 0 || z >= h->g.nz || (ez != 1 && ez != -1)) return FC_LBM_ERR_INVALID_ARG;
+    if (in_place(h)) return fail(h, FC_LBM_ERR_UNSUPPORTED, "layer copies need ping-pong streaming");
+    DeviceGuard dg(h->device);
+    const size_t elem = h->storage == FC_STORAGE_FP32 ? 4 : 2;
+    const size_t width = (size_t)h->g.nxy * elem, pitch = h->g.n * elem;
+    char* pop = static_cast<char*>(h->pop[next ? 1 - h->cur : h->cur]) + (size_t)z * width;
+    char* buf = static_cast<char*>(buffer);
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+    FC_RC(enter_stream(h, s));
+    if (!to_buffer) FC_RC(guard_snapshot(h, s, next ? 1 - h->cur : h->cur));
+    // one copy per plane with that e_z: FC_LBM_DIR_PLANES contiguous rows
+    int row = 0;
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < h->q && e == cudaSuccess; ++i) {
+        const int eiz = h->q == 19 ? fc::Lattice<19>::ez(i) : fc::Lattice<15>::ez(i);
+        if (eiz != ez) continue;
+        char* plane = pop + (size_t)i * pitch;
+        char* r = buf + (size_t)row * width;
+        e = to_buffer ? cudaMemcpyAsync(r, plane, width, cudaMemcpyDeviceToDevice, s)
+                      : cudaMemcpyAsync(plane, r, width, cudaMemcpyDeviceToDevice, s);
+        ++row;
+    }
+    FC_TRY(h, e, "layer copy");
+    if (row != FC_LBM_DIR_PLANES) return fail(h, FC_LBM_ERR_CUDA, "unexpected plane count per e_z");
     return leave_stream(h, s);
 }
 

@@ -103,6 +103,9 @@ struct ClosureDev {
     float inv_std[kClosureIn];
     float lo[3], hi[3];   // training range of inputs 0-2 (fallback outside)
     float filter_width;   // input 4
+    unsigned wall_min;    // wall-distance byte below which a cell keeps Smagorinsky (0: none)
+    float trust;          // > 0: 3 nu_t held in [ds / trust, ds * trust] around Smagorinsky's ds
+    float inv_trust;      // 1 / trust
 };
 
 // Host: packs FP32 weights (w1 [5][32], b1 [32], w2 [32][32], b2 [32], w3 [32],
@@ -119,12 +122,13 @@ void pack_closure_tc(const float* w1, const float* b1, const float* w2, const fl
 cudaError_t launch_wall_distance(const uint8_t* solid, const Geom& g, uint8_t* out, uint8_t* tmp, cudaStream_t s);
 
 // Training samples of the closure from a 2x box filter of this lattice
-// (closure.cu): rows (inputs 0-4, target nu_t) written to device `out` in
+// (closure.cu), a Smagorinsky run with tau_f and Cs cs_f: rows (inputs 0-4,
+// target nu_t) written to device `out` in
 // coarse cell order. Returns an FC_LBM_* status; *count is the sample count
 // (also when it exceeds `capacity`, FC_LBM_ERR_TOO_LARGE). Waits for `s`
 // (bounded: FC_LBM_ERR_TIMEOUT).
-int closure_samples(int q, int storage, const void* f, const uint8_t* solid, const Geom& fg, float tau_c,
-                    float filter_width, float* out, int64_t capacity, int64_t* count, cudaStream_t s);
+int closure_samples(int q, int storage, const void* f, const uint8_t* solid, const Geom& fg, float tau_f, float cs_f,
+                    float tau_c, float filter_width, float* out, int64_t capacity, int64_t* count, cudaStream_t s);
 
 // `tc`: the MLP on the tcgen05 tensor cores, once per block (closure_tc.cuh),
 // instead of the warp-level mma.sync MLP.

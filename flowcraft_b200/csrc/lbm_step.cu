@@ -392,9 +392,12 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned(const 
     // only in warps where some lane is still in range (warp votes, so the
     // branches stay uniform); the inputs are packed for the MLP only where
     // it runs.
+    // both cells' wall distances in one aligned load (x and nx are even)
+    const unsigned wd = pair ? (unsigned)__ldg(reinterpret_cast<const unsigned short*>(cl.wall + c)) : 0xffffu;
     float ra, rb;
     const float xa0 = closure_x0(mo.pp.x, mo.inv.x, ra), xb0 = closure_x0(mo.pp.y, mo.inv.y, rb);
-    bool la = closure_x0_in_range(cl, xa0), lb = closure_x0_in_range(cl, xb0);
+    bool la = closure_wall_ok(cl, wd & 0xffu) && closure_x0_in_range(cl, xa0);
+    bool lb = closure_wall_ok(cl, wd >> 8) && closure_x0_in_range(cl, xb0);
     float xa1 = 0.0f, xa2 = 0.0f, xb1 = 0.0f, xb2 = 0.0f;
     if (__any_sync(0xffffffffu, la || lb)) {
         closure_x12(mo.pxx.x, mo.pyy.x, mo.pzz.x, mo.pxy.x, mo.pxz.x, mo.pyz.x, ra, xa1, xa2);
@@ -403,10 +406,14 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned(const 
         lb = lb && closure_x12_in_range(cl, xb1, xb2);
     }
     // the Smagorinsky fallback only where some lane of the warp needs it
-    float sga = 0.0f, sgb = 0.0f;
-    if (__any_sync(0xffffffffu, !(la && lb))) {
+    float sga = 0.0f, sgb = 0.0f, dsa = 0.0f, dsb = 0.0f;
+    if (closure_anchored(cl) || __any_sync(0xffffffffu, !(la && lb))) {
         sga = smagorinsky_g(mo.pp.x, mo.rho.x, mo.inv.x, p.tau, p.cs);
         sgb = smagorinsky_g(mo.pp.y, mo.rho.y, mo.inv.y, p.tau, p.cs);
+        if (closure_anchored(cl)) {
+            dsa = smagorinsky_d3(mo.pp.x, mo.rho.x, mo.inv.x, p.tau, p.cs);
+            dsb = smagorinsky_d3(mo.pp.y, mo.rho.y, mo.inv.y, p.tau, p.cs);
+        }
     }
     // A cell outside the training range takes the Smagorinsky value, so a
     // warp with no cell in range has no use for the MLP and skips it (the
@@ -428,8 +435,6 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned(const 
     // row tiles of the MLP (8 lanes each) with a cell in range
     const unsigned tiles = ((need & 0xffu) ? 1u : 0u) | ((need & 0xff00u) ? 2u : 0u) |
                            ((need & 0xff0000u) ? 4u : 0u) | ((need & 0xff000000u) ? 8u : 0u);
-    // both cells' wall distances in one aligned load (x and nx are even)
-    const unsigned wd = pair ? (unsigned)__ldg(reinterpret_cast<const unsigned short*>(cl.wall + c)) : 0xffffu;
     uint32_t* in = &s_in[threadIdx.y][threadIdx.x * 8];
     closure_pack_inputs(cl, xa0, xa1, xa2, (float)(wd & 0xffu) * 0.0625f, in);
     closure_pack_inputs(cl, xb0, xb1, xb2, (float)(wd >> 8) * 0.0625f, in + 4);
@@ -441,8 +446,8 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned(const 
     mr.uy = sm[4 * 32], mr.uz = sm[5 * 32], mr.pxx = sm[6 * 32], mr.pyy = sm[7 * 32];
     mr.pzz = sm[8 * 32], mr.pxy = sm[9 * 32], mr.pxz = sm[10 * 32], mr.pyz = sm[11 * 32];
     float2 gr;
-    gr.x = la ? (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.x, p.tau))) * 4.5f : sga;
-    gr.y = lb ? (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.y, p.tau))) * 4.5f : sgb;
+    gr.x = la ? closure_g(cl, nu.x, p.tau, dsa) : sga;
+    gr.y = lb ? closure_g(cl, nu.y, p.tau, dsb) : sgb;
     relax2<Q>(v, mr, gr);
     if (bad) atomicOr(diverged, 1);
     store_pair<Q, S>(pp, c, v, pair);
@@ -528,7 +533,9 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned_tc(con
     // some lane is still in range (warp votes keep the branches uniform).
     float ra, rb;
     const float xa0 = closure_x0(mo.pp.x, mo.inv.x, ra), xb0 = closure_x0(mo.pp.y, mo.inv.y, rb);
-    bool la = row_ok && closure_x0_in_range(cl, xa0), lb = row_ok && closure_x0_in_range(cl, xb0);
+    const unsigned wd = pair ? (unsigned)__ldg(reinterpret_cast<const unsigned short*>(cl.wall + c)) : 0xffffu;
+    bool la = row_ok && closure_wall_ok(cl, wd & 0xffu) && closure_x0_in_range(cl, xa0);
+    bool lb = row_ok && closure_wall_ok(cl, wd >> 8) && closure_x0_in_range(cl, xb0);
     float xa1 = 0.0f, xa2 = 0.0f, xb1 = 0.0f, xb2 = 0.0f;
     if (__any_sync(0xffffffffu, la || lb)) {
         closure_x12(mo.pxx.x, mo.pyy.x, mo.pzz.x, mo.pxy.x, mo.pxz.x, mo.pyz.x, ra, xa1, xa2);
@@ -537,10 +544,14 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned_tc(con
         lb = lb && closure_x12_in_range(cl, xb1, xb2);
     }
     // the Smagorinsky fallback only where some lane of the warp needs it
-    float sga = 0.0f, sgb = 0.0f;
-    if (__any_sync(0xffffffffu, !(la && lb))) {
+    float sga = 0.0f, sgb = 0.0f, dsa = 0.0f, dsb = 0.0f;
+    if (closure_anchored(cl) || __any_sync(0xffffffffu, !(la && lb))) {
         sga = smagorinsky_g(mo.pp.x, mo.rho.x, mo.inv.x, p.tau, p.cs);
         sgb = smagorinsky_g(mo.pp.y, mo.rho.y, mo.inv.y, p.tau, p.cs);
+        if (closure_anchored(cl)) {
+            dsa = smagorinsky_d3(mo.pp.x, mo.rho.x, mo.inv.x, p.tau, p.cs);
+            dsb = smagorinsky_d3(mo.pp.y, mo.rho.y, mo.inv.y, p.tau, p.cs);
+        }
     }
     // A cell outside the training range takes the Smagorinsky value, so a
     // block with no cell in range has no use for the MLP and skips it (the
@@ -548,14 +559,12 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned_tc(con
     const bool live = __any_sync(0xffffffffu, la || lb);
     float2 g2 = make_float2(sga, sgb);
     if (__syncthreads_or(live)) {
-        // both cells' wall distances in one aligned load (x and nx are even)
-        const unsigned wd = pair ? (unsigned)__ldg(reinterpret_cast<const unsigned short*>(cl.wall + c)) : 0xffffu;
         uint4 ia, ib;
         closure_pack_inputs(cl, xa0, xa1, xa2, (float)(wd & 0xffu) * 0.0625f, reinterpret_cast<uint32_t*>(&ia));
         closure_pack_inputs(cl, xb0, xb1, xb2, (float)(wd >> 8) * 0.0625f, reinterpret_cast<uint32_t*>(&ib));
         const float2 nu = closure_cta_mlp(tsm, cl, ia, ib, live, diverged);
-        if (la) g2.x = (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.x, p.tau))) * 4.5f;
-        if (lb) g2.y = (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.y, p.tau))) * 4.5f;
+        if (la) g2.x = closure_g(cl, nu.x, p.tau, dsa);
+        if (lb) g2.y = closure_g(cl, nu.y, p.tau, dsb);
     }
     if (!pair) return;
     relax2<Q>(v, mo, g2);
@@ -610,8 +619,8 @@ __global__ void __launch_bounds__(128) k_closure_probe(const typename S::T* __re
     ib[3] = hb ? (float)cl.wall[c + 1] * 0.0625f : 0.0f;
     const int warp = threadIdx.x >> 5;
     if (!out) {
-        const bool ra = ha && closure_in_range(cl, ia[0], ia[1], ia[2]);
-        const bool rb = hb && closure_in_range(cl, ib[0], ib[1], ib[2]);
+        const bool ra = ha && closure_wall_ok(cl, cl.wall[c]) && closure_in_range(cl, ia[0], ia[1], ia[2]);
+        const bool rb = hb && closure_wall_ok(cl, cl.wall[c + 1]) && closure_in_range(cl, ib[0], ib[1], ib[2]);
         const unsigned cells = __popc(__ballot_sync(0xffffffffu, ra)) + __popc(__ballot_sync(0xffffffffu, rb));
         if ((threadIdx.x & 31) == 0 && cells) {
             atomicAdd(counts, (unsigned long long)cells);
@@ -627,12 +636,12 @@ __global__ void __launch_bounds__(128) k_closure_probe(const typename S::T* __re
     if (ha) {
         for (int k = 0; k < 4; ++k) out[5 * c + k] = ia[k];
         out[5 * c + 4] = nu.x;
-        in_range[c] = closure_in_range(cl, ia[0], ia[1], ia[2]) ? 1 : 0;
+        in_range[c] = closure_wall_ok(cl, cl.wall[c]) && closure_in_range(cl, ia[0], ia[1], ia[2]) ? 1 : 0;
     }
     if (hb) {
         for (int k = 0; k < 4; ++k) out[5 * (c + 1) + k] = ib[k];
         out[5 * (c + 1) + 4] = nu.y;
-        in_range[c + 1] = closure_in_range(cl, ib[0], ib[1], ib[2]) ? 1 : 0;
+        in_range[c + 1] = closure_wall_ok(cl, cl.wall[c + 1]) && closure_in_range(cl, ib[0], ib[1], ib[2]) ? 1 : 0;
     }
 }
 
@@ -963,8 +972,9 @@ __global__ void __launch_bounds__(128) k_boundary_pull_learned(const typename S:
     float x0, x1, x2;
     closure_invariants(mo.pxx.x, mo.pyy.x, mo.pzz.x, mo.pxy.x, mo.pxz.x, mo.pyz.x, mo.pp.x, mo.inv.x, x0, x1, x2);
     const float x3 = fluid ? (float)__ldg(cl.wall + c) * 0.0625f : 0.0f;
-    const bool lin = fluid && closure_in_range(cl, x0, x1, x2);
+    const bool lin = fluid && closure_wall_ok(cl, __ldg(cl.wall + c)) && closure_in_range(cl, x0, x1, x2);
     const float sg = smagorinsky_g(mo.pp.x, mo.rho.x, mo.inv.x, p.tau, p.cs);
+    const float ds = closure_anchored(cl) ? smagorinsky_d3(mo.pp.x, mo.rho.x, mo.inv.x, p.tau, p.cs) : 0.0f;
     const int warp = threadIdx.x >> 5;
     uint32_t* in = &s_in[warp][(threadIdx.x & 31) * 8];
     closure_pack_inputs(cl, x0, x1, x2, x3, in);
@@ -973,7 +983,7 @@ __global__ void __launch_bounds__(128) k_boundary_pull_learned(const typename S:
     float2 nu = make_float2(0.0f, 0.0f);  // warps with no cell in range skip the MLP
     if (__any_sync(0xffffffffu, lin)) nu = closure_warp_mlp(cl.frag, s_in[warp], s_out[warp]);
     if (!fluid) return;
-    const float gx = lin ? (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.x, p.tau))) * 4.5f : sg;
+    const float gx = lin ? closure_g(cl, nu.x, p.tau, ds) : sg;
     relax2<Q>(h, mo, make_float2(gx, gx));
     if (bad) atomicOr(diverged, 1);
     static_for<0, Q>([&](auto I) {

@@ -531,9 +531,12 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_aa_learned(typ
     const unsigned bad = moments2<Q>(v, mo) & pair;
     // the range test, the Smagorinsky fallback and the MLP as in
     // k_bulk_pairs_learned (warp votes keep every branch uniform)
+    // both cells' wall distances in one aligned load (x and nx are even)
+    const unsigned wd = pair ? (unsigned)__ldg(reinterpret_cast<const unsigned short*>(cl.wall + c)) : 0xffffu;
     float ra, rb;
     const float xa0 = closure_x0(mo.pp.x, mo.inv.x, ra), xb0 = closure_x0(mo.pp.y, mo.inv.y, rb);
-    bool la = closure_x0_in_range(cl, xa0), lb = closure_x0_in_range(cl, xb0);
+    bool la = closure_wall_ok(cl, wd & 0xffu) && closure_x0_in_range(cl, xa0);
+    bool lb = closure_wall_ok(cl, wd >> 8) && closure_x0_in_range(cl, xb0);
     float xa1 = 0.0f, xa2 = 0.0f, xb1 = 0.0f, xb2 = 0.0f;
     if (__any_sync(0xffffffffu, la || lb)) {
         closure_x12(mo.pxx.x, mo.pyy.x, mo.pzz.x, mo.pxy.x, mo.pxz.x, mo.pyz.x, ra, xa1, xa2);
@@ -541,10 +544,14 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_aa_learned(typ
         la = la && closure_x12_in_range(cl, xa1, xa2);
         lb = lb && closure_x12_in_range(cl, xb1, xb2);
     }
-    float sga = 0.0f, sgb = 0.0f;
-    if (__any_sync(0xffffffffu, !(la && lb))) {
+    float sga = 0.0f, sgb = 0.0f, dsa = 0.0f, dsb = 0.0f;
+    if (closure_anchored(cl) || __any_sync(0xffffffffu, !(la && lb))) {
         sga = smagorinsky_g(mo.pp.x, mo.rho.x, mo.inv.x, p.tau, p.cs);
         sgb = smagorinsky_g(mo.pp.y, mo.rho.y, mo.inv.y, p.tau, p.cs);
+        if (closure_anchored(cl)) {
+            dsa = smagorinsky_d3(mo.pp.x, mo.rho.x, mo.inv.x, p.tau, p.cs);
+            dsb = smagorinsky_d3(mo.pp.y, mo.rho.y, mo.inv.y, p.tau, p.cs);
+        }
     }
     const unsigned need = __ballot_sync(0xffffffffu, la || lb);
     if (!need) {
@@ -560,8 +567,6 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_aa_learned(typ
     sm[8 * 32] = mo.pzz, sm[9 * 32] = mo.pxy, sm[10 * 32] = mo.pxz, sm[11 * 32] = mo.pyz;
     const unsigned tiles = ((need & 0xffu) ? 1u : 0u) | ((need & 0xff00u) ? 2u : 0u) |
                            ((need & 0xff0000u) ? 4u : 0u) | ((need & 0xff000000u) ? 8u : 0u);
-    // both cells' wall distances in one aligned load (x and nx are even)
-    const unsigned wd = pair ? (unsigned)__ldg(reinterpret_cast<const unsigned short*>(cl.wall + c)) : 0xffffu;
     uint32_t* in = &s_in[threadIdx.y][threadIdx.x * 8];
     closure_pack_inputs(cl, xa0, xa1, xa2, (float)(wd & 0xffu) * 0.0625f, in);
     closure_pack_inputs(cl, xb0, xb1, xb2, (float)(wd >> 8) * 0.0625f, in + 4);
@@ -573,8 +578,8 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_aa_learned(typ
     mr.uy = sm[4 * 32], mr.uz = sm[5 * 32], mr.pxx = sm[6 * 32], mr.pyy = sm[7 * 32];
     mr.pzz = sm[8 * 32], mr.pxy = sm[9 * 32], mr.pxz = sm[10 * 32], mr.pyz = sm[11 * 32];
     float2 gr;
-    gr.x = la ? (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.x, p.tau))) * 4.5f : sga;
-    gr.y = lb ? (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.y, p.tau))) * 4.5f : sgb;
+    gr.x = la ? closure_g(cl, nu.x, p.tau, dsa) : sga;
+    gr.y = lb ? closure_g(cl, nu.y, p.tau, dsb) : sgb;
     relax2<Q>(v, mr, gr);
     if (bad) atomicOr(diverged, 1);
     aa_store_pair<Q, S, Odd>(f, pp, g, sd, v, c, x, y, z, row, pair, fast);
@@ -662,8 +667,9 @@ __global__ void __launch_bounds__(128) k_boundary_aa_learned(typename S::T* f, B
     float x0, x1, x2;
     closure_invariants(mo.pxx.x, mo.pyy.x, mo.pzz.x, mo.pxy.x, mo.pxz.x, mo.pyz.x, mo.pp.x, mo.inv.x, x0, x1, x2);
     const float x3 = fluid ? (float)__ldg(cl.wall + c) * 0.0625f : 0.0f;
-    const bool lin = fluid && closure_in_range(cl, x0, x1, x2);
+    const bool lin = fluid && closure_wall_ok(cl, __ldg(cl.wall + c)) && closure_in_range(cl, x0, x1, x2);
     const float sg = smagorinsky_g(mo.pp.x, mo.rho.x, mo.inv.x, p.tau, p.cs);
+    const float ds = closure_anchored(cl) ? smagorinsky_d3(mo.pp.x, mo.rho.x, mo.inv.x, p.tau, p.cs) : 0.0f;
     const int warp = threadIdx.x >> 5;
     uint32_t* in = &s_in[warp][(threadIdx.x & 31) * 8];
     closure_pack_inputs(cl, x0, x1, x2, x3, in);
@@ -672,7 +678,7 @@ __global__ void __launch_bounds__(128) k_boundary_aa_learned(typename S::T* f, B
     float2 nu = make_float2(0.0f, 0.0f);  // warps with no cell in range skip the MLP
     if (__any_sync(0xffffffffu, lin)) nu = closure_warp_mlp(cl.frag, s_in[warp], s_out[warp]);
     if (!fluid) return;
-    const float gx = lin ? (1.0f - __fdividef(1.0f, fmaf(3.0f, nu.x, p.tau))) * 4.5f : sg;
+    const float gx = lin ? closure_g(cl, nu.x, p.tau, ds) : sg;
     relax2<Q>(h, mo, make_float2(gx, gx));
     if (bad) atomicOr(diverged, 1);
     float vf[Q];

@@ -109,7 +109,8 @@ class _AeroForces(ctypes.Structure):
 class _Closure(ctypes.Structure):
     _fields_ = [("w1", _FPTR), ("b1", _FPTR), ("w2", _FPTR), ("b2", _FPTR), ("w3", _FPTR), ("b3", ctypes.c_float),
                 ("out_scale", ctypes.c_float), ("mean", ctypes.c_float * 5), ("std", ctypes.c_float * 5),
-                ("lo", ctypes.c_float * 3), ("hi", ctypes.c_float * 3), ("filter_width", ctypes.c_float)]
+                ("lo", ctypes.c_float * 3), ("hi", ctypes.c_float * 3), ("filter_width", ctypes.c_float),
+                ("min_wall_distance", ctypes.c_float), ("trust_factor", ctypes.c_float)]
 
 
 class _VoxelParams(ctypes.Structure):
@@ -159,6 +160,7 @@ SIGNATURES = {
     "fc_lbm_wall_distance": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint8), _SZ]),
     "fc_lbm_closure_coverage": (ctypes.c_int, [_P, _U64P, _U64P]),
     "fc_lbm_layer_copy": (ctypes.c_int, [_P, _I32, _I32, _P, _I32, _P]),
+    "fc_lbm_layer_copy_dir": (ctypes.c_int, [_P, _I32, _I32, _P, _I32, _I32, _P]),
     "fc_lbm_readback_field_async": (ctypes.c_int, [_P, _P, _SZ]),
     "fc_lbm_readback_wait": (ctypes.c_int, [_P, _I32]),
     "fc_lbm_alloc_pinned": (ctypes.c_int, [_SZ, ctypes.POINTER(ctypes.c_void_p)]),
@@ -457,6 +459,8 @@ class LbmSolver:
         c.lo[:] = [float(v) for v in weights.lo]
         c.hi[:] = [float(v) for v in weights.hi]
         c.filter_width = float(weights.filter_width)
+        c.min_wall_distance = float(getattr(weights, "wall_min", 0.0))
+        c.trust_factor = float(getattr(weights, "trust", 0.0))
         self._check(self._lib.fc_lbm_set_closure(self._h, ctypes.byref(c)), "SetClosure")
 
     def ClosureProbe(self):
@@ -510,10 +514,16 @@ class LbmSolver:
         self._check(self._lib.fc_lbm_readback_wait(self._h, int(timeout_ms)), "ReadbackWait")
         self._rb_out = None
 
-    def LayerCopy(self, z: int, buffer_ptr: int, to_buffer: bool, next_set: bool = False, cmd=None) -> None:
+    def LayerCopy(self, z: int, buffer_ptr: int, to_buffer: bool, next_set: bool = False, cmd=None,
+                  ez: int = 0) -> None:
         """Packs (to_buffer) or unpacks z-layer `z` of the current (or, with
         next_set, the in-progress step's output) population set to / from a
-        device buffer of Q*nx*ny elements."""
+        device buffer of Q*nx*ny elements; with ez = +1 or -1 only the 5
+        planes with that e_z, as the buffer's first 5 rows."""
+        if ez:
+            self._check(self._lib.fc_lbm_layer_copy_dir(self._h, int(z), int(next_set), buffer_ptr, int(to_buffer),
+                                                        int(ez), _stream_ptr(cmd)), "LayerCopy")
+            return
         self._check(self._lib.fc_lbm_layer_copy(self._h, int(z), int(next_set), buffer_ptr, int(to_buffer),
                                                 _stream_ptr(cmd)), "LayerCopy")
 

@@ -191,3 +191,30 @@ def aircraft(fuselage_length=400.0, span=360.0, root_chord=60.0, taper=0.6, cent
     fin = np.stack([fpos[:, 2] + cx, fpos[:, 1] + tail_y, fpos[:, 0] + cz + 0.5 * fr], axis=1)
     ftri = ftri.reshape(-1, 3)[:, [0, 2, 1]]  # the axis swap mirrors the winding
     return merge(fus, (wing[0], wing[1]), (htail[0], htail[1]), (fin, ftri))
+
+
+# The large configuration's aircraft: fuselage 400 cells long, wing span 360,
+# root chord 60 (taper 0.6), tessellated to 57,516 triangles, placed on a
+# 1024x512x512 lattice (scaled with nx) with the nose at 0.30 nx and the
+# fuselage axis on the lattice's y and z centre lines.
+C5_TESSELLATION = dict(n_chord=72, n_span=72, fuselage_res=(176, 88))
+
+
+def aircraft_c5(nx: int = 1024):
+    """(positions, indices) of the large configuration's aircraft mesh in
+    lattice units for an nx-long lattice (world y is the flow axis)."""
+    s = nx / 1024.0
+    return aircraft(fuselage_length=400.0 * s, span=360.0 * s, root_chord=60.0 * s, **C5_TESSELLATION)
+
+
+def aircraft_c5_origin(nx: int = 1024, ny: int = 512, nz: int = 512, z_lo: int = 0):
+    """World origin of the grid (cell size 1) that puts aircraft_c5(nx) where
+    the configuration places it. Cell (x, y, z) has its centre at world
+    (ox + y + 0.5, oy + x + 0.5, oz + z + 0.5) (grid x spans world y); the
+    fuselage centre sits at lattice coordinate (0.30 nx + 200 s, ny / 2,
+    nz / 2), s = nx / 1024, rounded to whole cells so that every cell centre
+    is exact in float (a grid over any sub-box then computes the same
+    centres). `z_lo`: origin of a slab whose first layer is lattice layer
+    z_lo."""
+    s = nx / 1024.0
+    return (-float(ny // 2), -float(round(0.30 * nx + 200.0 * s)), -float(nz // 2) + z_lo)

@@ -18,10 +18,17 @@ classified as in the whole lattice. A step goes:
   4. unpack the received layers into the output's inner halo layers;
   5. AdvanceSubstep.
 
+Only the planes that stream across the cut travel per step: the layer next
+to a lower halo reads from it the populations with e_z = +1 (the pull and
+the Bouzidi near-side partner alike), and the layer next to an upper halo
+those with e_z = -1, so each side sends 5 of the Q planes (D3Q19 and D3Q15)
+instead of all of them.
+
 The halo layers are never stepped (their content is what the neighbours
-send), so the owned layers are bit-identical to the unsplit lattice. The outer
-halo layers only feed readbacks of solid-cell forces: refresh() exchanges
-them, in the current population set, before such a readback.
+send), so the owned layers are bit-identical to the unsplit lattice. The
+halos' other planes, and the outer halo layers, only feed readbacks of
+solid-cell forces: refresh() exchanges both halo layers, all planes, in the
+current population set, before such a readback.
 
 The exchange is pluggable: NcclExchange (torch.distributed point-to-point on
 the device buffers, one process per GPU) and GlooExchange (CPU tensors, for
@@ -39,6 +46,7 @@ import contextlib
 from dataclasses import dataclass
 
 HALO = 2  # halo layers per side
+DIR_PLANES = 5  # planes with e_z = +1 (or -1), FC_LBM_DIR_PLANES
 
 
 def slab_ranges(nz: int, world: int):
@@ -96,15 +104,17 @@ def slab_stream(device: int):
 class SlabStepper:
     """The step sequence of one rank over any solver exposing
     StepRange(cmd, z0, zc), AdvanceSubstep() and LayerCopy(z, ptr,
-    to_buffer, next_set, cmd), with buffers given as (send_below,
+    to_buffer, next_set, cmd, ez), with buffers given as (send_below,
     recv_below, send_above, recv_above) objects whose ``ptr`` the solver
-    understands. With a torch stream ``cmd`` (from slab_stream), the
-    solver calls and the exchange all go on it."""
+    understands and whose ``tensor`` holds one row per plane. With a torch
+    stream ``cmd`` (from slab_stream), the solver calls and the exchange all
+    go on it. ``dir_rows``: the rows LayerCopy packs for one e_z direction."""
 
-    def __init__(self, solver, lay: SlabLayout, buffers, exchange, rank: int, cmd=None):
+    def __init__(self, solver, lay: SlabLayout, buffers, exchange, rank: int, cmd=None, dir_rows: int = DIR_PLANES):
         if cmd is not None and not getattr(cmd, "cuda_stream", 0):
             raise ValueError("the slab stream must be a non-default torch.cuda.Stream")
         self.s, self.lay, self.buf, self.ex, self.rank, self.cmd = solver, lay, buffers, exchange, rank, cmd
+        self.dir_rows = dir_rows
 
     def on_stream(self):
         """Makes cmd torch's current stream (for the exchange's copies and
@@ -123,23 +133,27 @@ class SlabStepper:
         k = 1 if outer else 0
         return self.lay.own0 - 1 - k, self.lay.own1 + k
 
-    def pack(self, outer: bool = False):
-        """The layers the neighbours need into the send buffers: the step's
-        output edges (inner), or the current set's second layers (outer)."""
+    def pack(self, outer: bool = False, full: bool = False):
+        """The layers the neighbours need into the send buffers. Per step
+        (neither flag): the step's output edges, only the planes streaming
+        across the cut (e_z = -1 down, +1 up). `full`: all planes of the
+        current set's edges (inner) or second layers (`outer`)."""
         lo, hi = self._send_layers(outer)
         send_lo, _, send_hi, _ = self.buf
+        step = not (outer or full)
         if self.lay.has_below:
-            self.s.LayerCopy(lo, send_lo.ptr, True, not outer, self.cmd)
+            self.s.LayerCopy(lo, send_lo.ptr, True, step, self.cmd, -1 if step else 0)
         if self.lay.has_above:
-            self.s.LayerCopy(hi, send_hi.ptr, True, not outer, self.cmd)
+            self.s.LayerCopy(hi, send_hi.ptr, True, step, self.cmd, 1 if step else 0)
 
-    def unpack(self, outer: bool = False):
+    def unpack(self, outer: bool = False, full: bool = False):
         lo, hi = self._recv_layers(outer)
         _, recv_lo, _, recv_hi = self.buf
+        step = not (outer or full)
         if self.lay.has_below:
-            self.s.LayerCopy(lo, recv_lo.ptr, False, not outer, self.cmd)
+            self.s.LayerCopy(lo, recv_lo.ptr, False, step, self.cmd, 1 if step else 0)
         if self.lay.has_above:
-            self.s.LayerCopy(hi, recv_hi.ptr, False, not outer, self.cmd)
+            self.s.LayerCopy(hi, recv_hi.ptr, False, step, self.cmd, -1 if step else 0)
 
     def edges(self):
         """Steps 1-2: the first and last owned layers, packed for the neighbours."""
@@ -160,14 +174,15 @@ class SlabStepper:
         self.unpack()
         self.s.AdvanceSubstep()
 
-    def posts(self):
-        """(peer, send buffer, receive buffer) pairs of this rank's exchange."""
+    def posts(self, rows=None):
+        """(peer, send, receive) of this rank's exchange: views of the
+        buffers' first `rows` rows (all rows when None)."""
         send_lo, recv_lo, send_hi, recv_hi = self.buf
         out = []
         if self.lay.has_below:
-            out.append((self.rank - 1, send_lo, recv_lo))
+            out.append((self.rank - 1, _Rows(send_lo, rows), _Rows(recv_lo, rows)))
         if self.lay.has_above:
-            out.append((self.rank + 1, send_hi, recv_hi))
+            out.append((self.rank + 1, _Rows(send_hi, rows), _Rows(recv_hi, rows)))
         return out
 
     def step(self, n: int = 1):
@@ -175,18 +190,26 @@ class SlabStepper:
         with self.on_stream():
             for _ in range(n):
                 self.edges()
-                h = self.ex.post(self.posts())
+                h = self.ex.post(self.posts(self.dir_rows))
                 self.interior()
                 self.ex.wait(h)
                 self.finish()
 
     def refresh(self):
-        """The outer halo layers of the current set (one process per rank),
-        before a readback of solid-cell forces."""
+        """Both halo layers of the current set, all planes (one process per
+        rank), before a readback of solid-cell forces."""
         with self.on_stream():
-            self.pack(outer=True)
-            self.ex.wait(self.ex.post(self.posts()))
-            self.unpack(outer=True)
+            for outer in (False, True):
+                self.pack(outer=outer, full=True)
+                self.ex.wait(self.ex.post(self.posts()))
+                self.unpack(outer=outer, full=True)
+
+
+class _Rows:
+    """The leading rows of an exchange buffer, as the exchange sends them."""
+
+    def __init__(self, buf, rows=None):
+        self.tensor = buf.tensor if rows is None else buf.tensor[:rows]
 
 
 class NcclExchange:
@@ -224,20 +247,21 @@ class GlooExchange:
 
 
 class DeviceBuffer:
-    """A device byte buffer for one packed layer (Q * nx * ny elements)."""
+    """A device byte buffer for one packed layer: `rows` planes of
+    `row_bytes` (nx * ny elements) each."""
 
-    def __init__(self, nbytes: int, device: int):
+    def __init__(self, rows: int, row_bytes: int, device: int):
         import torch
-        self.tensor = torch.empty(nbytes, dtype=torch.uint8, device=f"cuda:{device}")
+        self.tensor = torch.empty((rows, row_bytes), dtype=torch.uint8, device=f"cuda:{device}")
         self.ptr = self.tensor.data_ptr()
 
 
-def _copy_emulated(steppers):
+def _copy_emulated(steppers, rows=None):
     for st in steppers:
-        for peer, _send, recv in st.posts():
+        for peer, _send, recv in st.posts(rows):
             other = steppers[peer]
             # the peer's send buffer facing this rank
-            src = other.buf[0] if peer > st.rank else other.buf[2]
+            src = _Rows(other.buf[0] if peer > st.rank else other.buf[2], rows)
             recv.tensor.copy_(src.tensor)
 
 
@@ -256,7 +280,7 @@ def step_emulated(steppers, n: int = 1):
         for _ in range(n):
             for st in steppers:
                 st.edges()
-            _copy_emulated(steppers)
+            _copy_emulated(steppers, steppers[0].dir_rows)
             for st in steppers:
                 st.interior()
                 st.finish()
@@ -265,11 +289,12 @@ def step_emulated(steppers, n: int = 1):
 def refresh_emulated(steppers):
     """SlabStepper.refresh for ranks emulated in one process."""
     with _shared_stream(steppers):
-        for st in steppers:
-            st.pack(outer=True)
-        _copy_emulated(steppers)
-        for st in steppers:
-            st.unpack(outer=True)
+        for outer in (False, True):
+            for st in steppers:
+                st.pack(outer=outer, full=True)
+            _copy_emulated(steppers)
+            for st in steppers:
+                st.unpack(outer=outer, full=True)
 
 
 def make_slab_solver(solid, sdf, rank: int, world: int, device: int, model, storage, params, seed_mid=True,
@@ -299,9 +324,8 @@ def make_slab_solver(solid, sdf, rank: int, world: int, device: int, model, stor
     s.Reset(params, seed_mid)
     q = 19 if model == LatticeModel.D3Q19 else 15
     elem = 4 if storage == Storage.FP32 else 2
-    nbytes = q * nx * ny * elem
     with torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext():
-        bufs = tuple(DeviceBuffer(nbytes, device) for _ in range(4))
+        bufs = tuple(DeviceBuffer(q, nx * ny * elem, device) for _ in range(4))
     return s, lay, bufs
 
 

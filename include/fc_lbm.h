@@ -277,6 +277,8 @@ typedef struct fc_closure {
     float std[FC_CLOSURE_INPUTS];
     float lo[3], hi[3];            /* training range of inputs 0-2 */
     float filter_width;            /* input 4 for this lattice */
+    float min_wall_distance;       /* cells nearer a wall than this (in cells) keep Smagorinsky; 0 = none */
+    float trust_factor;            /* 0 = off; k >= 1: 3 nu_t held in [d/k, d k], d = 3 nu_t of Smagorinsky */
 } fc_closure;
 
 /* Installs the closure (copied; NULL returns to Smagorinsky) for every later
@@ -303,9 +305,12 @@ FC_LBM_API int fc_lbm_wall_distance(fc_lbm* h, uint8_t* out, size_t cells);
  * coarse cell off the faces and the inlet/outlet planes whose 6 neighbours
  * are fluid gives one row of 6 floats (inputs 0-4 and the target nu_t),
  * written to the DEVICE array `out` in coarse-cell order. The target is the
- * least-squares eddy viscosity of the sub-grid stress of the filtered flow
- * against its resolved strain (central differences); the inputs are those
- * of a coarse cell relaxing with the coarse molecular tau plus 3 nu_t.
+ * eddy viscosity that carries the filtered flow's stress: the least-squares
+ * fit of the box-filtered viscous stress of the fine cells (molecular plus
+ * this lattice's Smagorinsky, at its tau and Cs) minus the resolved sub-grid
+ * stress, against the filtered strain (central differences), less the coarse
+ * molecular viscosity, clipped at 0; the inputs are those of a coarse cell
+ * relaxing with the coarse molecular tau plus 3 nu_t.
  * *count receives the number of rows; with out NULL or capacity too small
  * nothing is written (FC_LBM_ERR_TOO_LARGE when rows did not fit). Blocking.
  * No reference counterpart. */
@@ -337,6 +342,15 @@ FC_LBM_API int fc_lbm_mlp_adam(float* params, const float* grad, float* m, float
  * `stream`. The halo exchange of a lattice split into z-slabs across GPUs
  * (flowcraft_b200/shard.py) is built on it; no reference counterpart. */
 FC_LBM_API int fc_lbm_layer_copy(fc_lbm* h, int32_t z, int32_t next, void* buffer, int32_t to_buffer, void* stream);
+/* The same for the planes whose e_z equals `ez` only (+1 or -1; 0 = all Q
+ * planes, as fc_lbm_layer_copy): their rows, in plane order, are the first
+ * FC_LBM_DIR_PLANES rows of the buffer. A step of the layer next to a halo
+ * reads only the halo's planes that stream toward it (e_z = +1 from the
+ * layer below, -1 from the layer above), so a per-step halo exchange moves 5
+ * of the Q planes. No reference counterpart. */
+#define FC_LBM_DIR_PLANES 5
+FC_LBM_API int fc_lbm_layer_copy_dir(fc_lbm* h, int32_t z, int32_t next, void* buffer, int32_t to_buffer, int32_t ez,
+                                     void* stream);
 
 /* ---- Asynchronous field readback (overlapped with stepping) ----
  * What FlowCraft's ReadbackFieldPacedGPU (main.cpp:2506-2555) does with

@@ -83,6 +83,8 @@ typedef struct {
     int closure_on;
     float cw1[5 * 32], cb1[32], cw2[32 * 32], cb2[32], cw3[32], cb3;
     float cmean[5], cinv_std[5], clo[3], chi[3], cfilter;
+    int cwall_min;  /* wall-distance byte below which a cell keeps Smagorinsky */
+    float ctrust;   /* > 0: 3 nu_t held within [d / ctrust, d * ctrust] of Smagorinsky's d */
     uint8_t* wall;
 } oracle_lbm;
 
@@ -410,11 +412,14 @@ static float bf16r(float x) {
 /* Installs the closure: the weights as the library packs them (BF16 weights
  * and hidden-layer biases, out_scale folded into the last layer, FP32 output
  * bias), the input
- * normalization and training range, and the wall distance (computed here
- * when `wall` is NULL). w1 NULL turns the closure off. */
+ * normalization and training range, the wall distance (computed here
+ * when `wall` is NULL), the near-wall fallback distance `wall_min` (cells)
+ * and the Smagorinsky trust factor `trust` (0: off). w1 NULL turns the
+ * closure off. */
 int SYM(set_closure)(oracle_lbm* o, const float* w1, const float* b1, const float* w2, const float* b2,
                      const float* w3, float b3, float out_scale, const float* mean, const float* std,
-                     const float* lo, const float* hi, float filter_width, const uint8_t* wall) {
+                     const float* lo, const float* hi, float filter_width, const uint8_t* wall, float wall_min,
+                     float trust) {
     if (!w1) {
         o->closure_on = 0;
         return 0;
@@ -436,6 +441,11 @@ int SYM(set_closure)(oracle_lbm* o, const float* w1, const float* b1, const floa
         o->chi[k] = hi[k];
     }
     o->cfilter = filter_width;
+    {
+        float wm = ceilf(wall_min * 16.0f);
+        o->cwall_min = wm > 255.0f ? 256 : (int)wm;
+    }
+    o->ctrust = trust;
     if (!o->wall) o->wall = (uint8_t*)malloc(o->n ? o->n : 1);
     if (wall)
         memcpy(o->wall, wall, o->n);
@@ -464,6 +474,7 @@ static float closure_nu(const oracle_lbm* o, const float* x3) {
     float x[5] = {x3[0], x3[1], x3[2], x3[3], o->cfilter};
     for (int k = 0; k < 3; ++k)
         if (!(x[k] >= o->clo[k] && x[k] <= o->chi[k])) return -1.0f;
+    if ((int)(x3[3] * 16.0f) < o->cwall_min) return -1.0f; /* near-wall fallback */
     float a[5], h1[32], h2[32];
     for (int k = 0; k < 5; ++k) a[k] = bf16r((x[k] - o->cmean[k]) * o->cinv_std[k]);
     for (int j = 0; j < 32; ++j) {
@@ -581,7 +592,15 @@ static void step_body(oracle_lbm* o, int z0, int z1, int tid, void* vctx) {
                     closure_inputs(pxx, pyy, pzz, pxy, pxz, pyz, rho, xin);
                     xin[3] = (float)o->wall[c] * 0.0625f;
                     float nu = closure_nu(o, xin);
-                    if (nu >= 0.0f) tau_eff = o->tau + K(3.0) * (real)nu;
+                    if (nu >= 0.0f) {
+                        real d = K(3.0) * (real)nu;
+                        if (o->ctrust > 0.0f) { /* anchored to Smagorinsky's 3 nu_t */
+                            real ds = tau_eff - o->tau;
+                            real dlo = ds / (real)o->ctrust, dhi = ds * (real)o->ctrust;
+                            d = d < dlo ? dlo : (d > dhi ? dhi : d);
+                        }
+                        tau_eff = o->tau + d;
+                    }
                 }
                 real omega = K(1.0) / tau_eff;
                 for (int i = 0; i < q; ++i) {

@@ -121,7 +121,7 @@ def _lib(precision: str):
     if not is_ref:
         u8p = ctypes.POINTER(ctypes.c_uint8)
         api["set_closure"] = fn("set_closure", c_int, vp, fptr, fptr, fptr, fptr, fptr, ctypes.c_float, ctypes.c_float,
-                                fptr, fptr, fptr, fptr, ctypes.c_float, u8p)
+                                fptr, fptr, fptr, fptr, ctypes.c_float, u8p, ctypes.c_float, ctypes.c_float)
         api["closure_eval"] = fn("closure_eval", None, vp, fptr, c_size, fptr)
         api["wall_distance"] = fn("wall_distance", None, c_int, c_int, c_int, u8p, u8p)
         api["readback_field_f64"] = fn("readback_field_f64", None, vp, ctypes.POINTER(ctypes.c_double))
@@ -205,7 +205,8 @@ class Oracle:
         flowcraft_b200.closure.ClosureWeights), or None for Smagorinsky."""
         fp = ctypes.POINTER(ctypes.c_float)
         if cw is None:
-            self.api["set_closure"](self.h, None, None, None, None, None, 0.0, 0.0, None, None, None, None, 0.0, None)
+            self.api["set_closure"](self.h, None, None, None, None, None, 0.0, 0.0, None, None, None, None, 0.0, None,
+                                    0.0, 0.0)
             return
         self._closure_keep = [np.ascontiguousarray(a, dtype=np.float32) for a in
                               (cw.w1, cw.b1, cw.w2, cw.b2, cw.w3, cw.mean, cw.std, cw.lo, cw.hi)]
@@ -215,7 +216,8 @@ class Oracle:
             self._wall = np.ascontiguousarray(wall, dtype=np.uint8).ravel()
             wl = self._wall.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
         self.api["set_closure"](self.h, k[0], k[1], k[2], k[3], k[4], float(cw.b3), float(cw.out_scale), k[5], k[6],
-                                k[7], k[8], float(cw.filter_width), wl)
+                                k[7], k[8], float(cw.filter_width), wl, float(getattr(cw, "wall_min", 0.0)),
+                                float(getattr(cw, "trust", 0.0)))
 
     def closure_eval(self, inputs) -> np.ndarray:
         """nu_t (-1 outside the training range) for rows of inputs 0-3."""

@@ -1,23 +1,33 @@
-"""Precision study (the 384x192x192 NACA 0012 precision configuration at
-half size): the GPU storage formats and the learned closure against the FP64
-oracle, and the learned closure's drag and lift against the FP32 Smagorinsky
-GPU run.
+"""Precision study of the storage formats (the 384x192x192 NACA 0012
+precision configuration): the GPU's FP32, FP16-offset and BF16-offset
+storage, and FP16 with the learned closure, against the FP64 oracle, on
+D3Q19 and D3Q15.
 
-Case: NACA 0012 wing, chord 48, span 64, 4 deg, on 192x96x96 (the full-size
-case halved, so nu and tau are the full-size case's: U 0.06, Re 5e3 on the
-chord, tau 0.50173), Smagorinsky Cs 0.1, mid-speed seed, 1000 steps, D3Q19
-and D3Q15. Drag and lift are the x and z sums of the solid cells'
-momentum-exchange force (the device FP64 integral), normalized by
-0.5 rho U^2 chord span.
+Case: NACA 0012 wing, chord 96, span 128, 4 deg, on 384x192x192 (14.2M
+cells), U 0.06, Re 1e4 on the chord (tau 0.50173), mid-speed seed, 5000
+steps. D3Q19 runs at Smagorinsky Cs 0.1. D3Q15 is less stable at this
+viscosity and runs at the larger Cs that DESIGN's precision section names
+(D3Q15_CS below), the smallest of the probed values at which the run stays
+finite for all 5000 steps. Drag and lift are the x and z sums of the
+solid cells' momentum-exchange force, normalized by 0.5 rho U^2 chord
+span, averaged every 10 steps over the last fifth of the run.
 
-Not collected by pytest; run on a GPU machine:  python tests/precision_study.py
-It prints one JSON object and a markdown table. Cd and Cl are reported at
-the last step and averaged over the last fifth of the steps (as the polar
-sweep averages them). STUDY_GPU_ONLY=1 skips the FP64 oracle runs and
-compares the GPU variants with each other only.
+The oracle runs take hours of host CPU and the GPU runs seconds, so the
+study runs in three phases that share a directory (not collected by
+pytest):
+
+  python tests/precision_study.py oracle --lattice 19 --out DIR   (host CPU)
+  python tests/precision_study.py gpu --out DIR                   (a B200)
+  python tests/precision_study.py compare --out DIR
+
+Fields are compared on every 4th cell along each axis (96x48x48 cells, the
+fluid ones), which keeps the GPU phase's output small; forces use the whole
+lattice. ``--half`` runs the same case at half size (192x96x96, chord 48,
+span 64, the same tau) for 1000 steps.
 """
 from __future__ import annotations
 
+import argparse
 import json
 import os
 import sys
@@ -28,118 +38,167 @@ import numpy as np
 ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
 sys.path.insert(0, ROOT)
 
-NX, NY, NZ, CHORD, SPAN, AOA, U = 192, 96, 96, 48.0, 64.0, 4.0, 0.06
-STEPS = int(os.environ.get("STUDY_STEPS", "1000"))
-AVG_FROM = STEPS - STEPS // 5
-GPU_ONLY = os.environ.get("STUDY_GPU_ONLY", "0") == "1"
-TAU = 0.5 + 3.0 * U * CHORD / 5e3
-CS = 0.1
+U = 0.06
+D3Q19_CS = 0.1
+D3Q15_CS = 0.2
+SUB = 4  # field comparison on every SUB-th cell per axis
 
 
-def geometry():
+def case(half: bool):
+    if half:
+        return dict(nx=192, ny=96, nz=96, chord=48.0, span=64.0, aoa=4.0, steps=1000)
+    return dict(nx=384, ny=192, nz=192, chord=96.0, span=128.0, aoa=4.0, steps=5000)
+
+
+def tau_of(c):
+    return 0.5 + 3.0 * U * 96.0 / 1e4  # the full-size case's viscosity at either size
+
+
+def cs_of(q):
+    return D3Q19_CS if q == 19 else D3Q15_CS
+
+
+def geometry(c):
     from flowcraft_b200 import geometry as geo
-    solid, sdf = geo.naca_wing_grid(NX, NY, NZ, chord=CHORD, span=SPAN, aoa_deg=AOA, digits="0012")
+    solid, sdf = geo.naca_wing_grid(c["nx"], c["ny"], c["nz"], chord=c["chord"], span=c["span"], aoa_deg=c["aoa"],
+                                    digits="0012")
     return np.ascontiguousarray(solid, np.uint8), np.ascontiguousarray(sdf, np.float32)
 
 
-def coeffs(force):
-    q = 0.5 * U * U * CHORD * SPAN
-    return force[0] / q, force[2] / q
+def coeffs(force, c):
+    q = 0.5 * U * U * c["chord"] * c["span"]
+    return float(force[0] / q), float(force[2] / q)
 
 
-def run_oracle(solid, sdf, q, closure=None):
+def subsample(field, c):
+    f = np.asarray(field).reshape(c["nz"], c["ny"], c["nx"], 4)
+    return np.ascontiguousarray(f[::SUB, ::SUB, ::SUB])
+
+
+def run_oracle(c, q, threads, out):
     from oracle import oracle as orc
-    p = orc.Params(TAU, U, False, True, True, CS)
-    o = orc.Oracle(solid, sdf, q, p, seed_mid=True, precision="f64")
-    if closure is not None:
-        o.set_closure(closure)
-    o.step(STEPS)
-    f = o.readback_field_f64().reshape(-1, 4)
-    o.close()
+    solid, sdf = geometry(c)
+    p = orc.Params(tau_of(c), U, False, True, True, cs_of(q))
+    o = orc.Oracle(solid, sdf, q, p, seed_mid=True, precision="f64", threads=threads)
+    steps = c["steps"]
+    avg_from = steps - steps // 5
+    t0 = time.time()
+    o.step(avg_from)
+    acc, n = np.zeros(3), 0
     s = solid.ravel().astype(bool)
-    force = f[s][:, 1:4].sum(axis=0)
-    return f, force
+    f = None
+    for _ in range(avg_from, steps, 10):
+        o.step(10)
+        f = o.readback_field_f64().reshape(-1, 4)
+        acc += f[s][:, 1:4].sum(axis=0)
+        n += 1
+    np.savez(os.path.join(out, f"fp64_q{q}.npz"), sub=subsample(f, c), force=f[s][:, 1:4].sum(axis=0),
+             force_avg=acc / n, diverged=o.has_diverged(), seconds=time.time() - t0)
+    o.close()
 
 
-def run_gpu(solid, sdf, q, storage, closure=None):
+def run_gpu_variant(c, q, storage, closure, solid, sdf):
     from flowcraft_b200.lbm import LatticeModel, LbmSolver, Params, Storage, VoxelGrid
     s = LbmSolver()
-    g = VoxelGrid(NX, NY, NZ, solid=solid.ravel(), signedDistance=sdf.ravel())
+    g = VoxelGrid(c["nx"], c["ny"], c["nz"], solid=solid.ravel(), signedDistance=sdf.ravel())
     assert s.Init(0, g, LatticeModel.D3Q19 if q == 19 else LatticeModel.D3Q15, Storage[storage]), s.LastError()
-    s.Reset(Params(tau=TAU, inletVelocity=U, smagorinskyCs=CS), True)
+    s.Reset(Params(tau=tau_of(c), inletVelocity=U, smagorinskyCs=cs_of(q)), True)
     if closure is not None:
         s.SetClosure(closure)
-    s.Step(None, AVG_FROM)
+    steps = c["steps"]
+    avg_from = steps - steps // 5
+    s.Step(None, avg_from)
     acc, n = np.zeros(3), 0
-    for _ in range(AVG_FROM, STEPS, 10):
+    for _ in range(avg_from, steps, 10):
         s.Step(None, 10)
         acc += np.asarray(s.AerodynamicForces().forceSum)
         n += 1
-    f = s.ReadbackField().reshape(-1, 4).astype(np.float64)
-    a = s.AerodynamicForces()
+    f = s.ReadbackField()
+    force = np.asarray(s.AerodynamicForces().forceSum)
+    diverged = s.HasDiverged()
     s.close()
-    return f, np.asarray(a.forceSum), acc / max(n, 1)
+    return dict(sub=subsample(f, c), force=force, force_avg=acc / n, diverged=diverged)
 
 
-def errors(f, ref, solid):
-    fl = ~solid.ravel().astype(bool)
-    d = np.abs(f - ref)[fl]
-    ua, ub = np.linalg.norm(f[fl][:, 1:], axis=1), np.linalg.norm(ref[fl][:, 1:], axis=1)
-    return {"max_drho": float(d[:, 0].max()), "max_du": float(np.abs(ua - ub).max()),
-            "rms_du": float(np.sqrt(np.mean((ua - ub) ** 2))), "umax": float(ub.max())}
-
-
-def main():
+def run_gpu(c, out):
     from flowcraft_b200.closure import ClosureWeights
     cw = ClosureWeights.load(os.path.join(ROOT, "flowcraft_b200", "data", "closure_c4.json"))
-    solid, sdf = geometry()
-    out = {"case": f"NACA 0012 {NX}x{NY}x{NZ}, chord {CHORD}, span {SPAN}, {AOA} deg, U {U}, tau {TAU:.5f}, "
-                   f"Cs {CS}, {STEPS} steps, forces averaged over steps {AVG_FROM}-{STEPS}", "rows": []}
-    for q in ((19,) if GPU_ONLY else (19, 15)):
-        t0 = time.time()
-        if not GPU_ONLY:
-            ref, fref = run_oracle(solid, sdf, q)
-            cd0, cl0 = coeffs(fref)
-            refl, frefl = (run_oracle(solid, sdf, q, cw) if q == 19 else (None, None))
-        t1 = time.time()
-        gpu = {st: run_gpu(solid, sdf, q, st) for st in ("FP32", "FP16_OFFSET", "BF16_OFFSET")}
-        if q == 19:
-            gpu["FP16_OFFSET+learned"] = run_gpu(solid, sdf, q, "FP16_OFFSET", cw)
-        cd32, cl32 = coeffs(gpu["FP32"][1])
-        acd32, acl32 = coeffs(gpu["FP32"][2])
-        for name, (f, force, avg) in gpu.items():
-            learned = name.endswith("learned")
-            cd, cl = coeffs(force)
-            acd, acl = coeffs(avg)
-            row = {"lattice": f"D3Q{q}", "variant": name, "Cd": cd, "Cl": cl, "Cd_avg": acd, "Cl_avg": acl,
-                   "dCd_rel_fp32_smag": (cd - cd32) / abs(cd32), "dCl_rel_fp32_smag": (cl - cl32) / abs(cl32),
-                   "dCd_avg_rel_fp32_smag": (acd - acd32) / abs(acd32),
-                   "dCl_avg_rel_fp32_smag": (acl - acl32) / abs(acl32)}
-            if not GPU_ONLY:
-                r = refl if learned else ref
-                fr = frefl if learned else fref
-                cdr, clr = coeffs(fr)
-                row.update({"reference": "FP64 oracle" + (" + same closure" if learned else ""),
-                            **errors(f, r, solid), "Cd_fp64": cdr, "Cl_fp64": clr,
-                            "dCd_rel_fp64": (cd - cdr) / abs(cdr), "dCl_rel_fp64": (cl - clr) / abs(clr)})
-            out["rows"].append(row)
-        if not GPU_ONLY:
-            out[f"oracle_seconds_q{q}"] = round(t1 - t0, 1)
-            out[f"fp64_smagorinsky_q{q}"] = {"Cd": cd0, "Cl": cl0}
-    print(json.dumps(out))
-    print("\n| lattice | variant | Cd | Cl | dCd vs FP32 Smag | dCl vs FP32 Smag | Cd avg | Cl avg | "
-          "dCd avg vs FP32 Smag | dCl avg vs FP32 Smag |")
-    print("|---|---|---|---|---|---|---|---|---|---|")
-    for r in out["rows"]:
-        print(f"| {r['lattice']} | {r['variant']} | {r['Cd']:.5f} | {r['Cl']:.5f} | "
-              f"{100 * r['dCd_rel_fp32_smag']:+.3f} % | {100 * r['dCl_rel_fp32_smag']:+.3f} % | {r['Cd_avg']:.5f} | "
-              f"{r['Cl_avg']:.5f} | {100 * r['dCd_avg_rel_fp32_smag']:+.3f} % | {100 * r['dCl_avg_rel_fp32_smag']:+.3f} % |")
-    if not GPU_ONLY:
-        print("\n| lattice | variant | max|drho| | max|du| | rms|du| | dCd vs FP64 | dCl vs FP64 |")
-        print("|---|---|---|---|---|---|---|")
-        for r in out["rows"]:
-            print(f"| {r['lattice']} | {r['variant']} | {r['max_drho']:.2e} | {r['max_du']:.2e} | {r['rms_du']:.2e} | "
-                  f"{100 * r['dCd_rel_fp64']:+.3f} % | {100 * r['dCl_rel_fp64']:+.3f} % |")
+    solid, sdf = geometry(c)
+    for q in (19, 15):
+        for name, storage, closure in (("FP32", "FP32", None), ("FP16_OFFSET", "FP16_OFFSET", None),
+                                       ("BF16_OFFSET", "BF16_OFFSET", None),
+                                       ("FP16_OFFSET+learned", "FP16_OFFSET", cw)):
+            if closure is not None and q != 19:
+                continue
+            t0 = time.time()
+            r = run_gpu_variant(c, q, storage, closure, solid, sdf)
+            np.savez(os.path.join(out, f"gpu_q{q}_{name}.npz"), seconds=time.time() - t0, **r)
+            print(f"D3Q{q} {name}: diverged={r['diverged']} {time.time() - t0:.1f}s", flush=True)
+
+
+def errors(sub, ref, solid_sub):
+    fl = ~solid_sub.astype(bool).ravel()
+    a, b = sub.reshape(-1, 4)[fl].astype(np.float64), ref.reshape(-1, 4)[fl]
+    ua, ub = np.linalg.norm(a[:, 1:], axis=1), np.linalg.norm(b[:, 1:], axis=1)
+    return {"max_drho": float(np.abs(a[:, 0] - b[:, 0]).max()), "max_du": float(np.abs(ua - ub).max()),
+            "rms_du": float(np.sqrt(np.mean((ua - ub) ** 2))), "umax": float(ub.max()), "cells": int(fl.sum())}
+
+
+def compare(c, out):
+    solid, _ = geometry(c)
+    solid_sub = solid[::SUB, ::SUB, ::SUB]
+    rows = []
+    for q in (19, 15):
+        ref_path = os.path.join(out, f"fp64_q{q}.npz")
+        ref = np.load(ref_path) if os.path.exists(ref_path) else None
+        g32 = np.load(os.path.join(out, f"gpu_q{q}_FP32.npz"))
+        acd32, acl32 = coeffs(g32["force_avg"], c)
+        for name in ("FP32", "FP16_OFFSET", "BF16_OFFSET", "FP16_OFFSET+learned"):
+            path = os.path.join(out, f"gpu_q{q}_{name}.npz")
+            if not os.path.exists(path):
+                continue
+            g = np.load(path)
+            cd, cl = coeffs(g["force_avg"], c)
+            row = {"lattice": f"D3Q{q}", "Cs": cs_of(q), "variant": name, "diverged": bool(g["diverged"]),
+                   "Cd_avg": cd, "Cl_avg": cl, "dCd_vs_fp32_smag": cd / acd32 - 1.0,
+                   "dCl_vs_fp32_smag": cl / acl32 - 1.0}
+            if ref is not None:
+                rcd, rcl = coeffs(ref["force_avg"], c)
+                row.update(errors(g["sub"], ref["sub"], solid_sub))
+                row.update({"Cd_fp64": rcd, "Cl_fp64": rcl, "dCd_vs_fp64": cd / rcd - 1.0,
+                            "dCl_vs_fp64": cl / rcl - 1.0, "fp64_diverged": bool(ref["diverged"]),
+                            "reference": "FP64 oracle, Smagorinsky"})
+            rows.append(row)
+    res = {"case": {**c, "tau": tau_of(c), "U": U, "sub": SUB}, "rows": rows}
+    print(json.dumps(res))
+    print("\n| lattice (Cs) | variant | max abs drho | max abs d|u| | rms d|u| | Cd avg | Cl avg | dCd vs FP64 | "
+          "dCl vs FP64 | dCd vs FP32 Smag | dCl vs FP32 Smag |")
+    print("|---|---|---|---|---|---|---|---|---|---|---|")
+    for r in rows:
+        e = (f"{r['max_drho']:.1e} | {r['max_du']:.1e} | {r['rms_du']:.1e}" if "max_drho" in r else "- | - | -")
+        f64 = (f"{100 * r['dCd_vs_fp64']:+.2f} % | {100 * r['dCl_vs_fp64']:+.2f} %" if "dCd_vs_fp64" in r
+               else "- | -")
+        print(f"| {r['lattice']} ({r['Cs']}) | {r['variant']} | {e} | {r['Cd_avg']:.5f} | {r['Cl_avg']:.5f} | {f64} | "
+              f"{100 * r['dCd_vs_fp32_smag']:+.2f} % | {100 * r['dCl_vs_fp32_smag']:+.2f} % |")
+    return res
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("phase", choices=["oracle", "gpu", "compare"])
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--lattice", type=int, default=19, choices=[19, 15])
+    ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--half", action="store_true")
+    a = ap.parse_args(argv)
+    os.makedirs(a.out, exist_ok=True)
+    c = case(a.half)
+    if a.phase == "oracle":
+        run_oracle(c, a.lattice, a.threads, a.out)
+    elif a.phase == "gpu":
+        run_gpu(c, a.out)
+    else:
+        compare(c, a.out)
 
 
 if __name__ == "__main__":

@@ -47,8 +47,11 @@ def test_mlp_grad_forward_adam_match_oracle(gpu):
     assert np.abs(tr.params() - (p - step)).max() < 2e-6
 
 
-def _box_filter_samples(pops, solid, tau_c, filter_width):
-    """Restatement of the sample extraction in float64 numpy (closure.cu)."""
+def _box_filter_samples(pops, solid, tau_c, filter_width, tau_f, cs_f):
+    """Restatement of the sample extraction in float64 numpy (closure.cu):
+    the target fits the filtered viscous stress (each fine cell's relaxation
+    time recovered from its post-collision stress) minus the resolved
+    sub-grid stress."""
     from test_closure_gpu import LATTICE
     e = np.asarray(LATTICE[pops.shape[0]], np.float64)
     nz, ny, nx = solid.shape
@@ -68,6 +71,15 @@ def _box_filter_samples(pops, solid, tau_c, filter_width):
     rb = rs / 8.0
     uu = blk(np.einsum("zyx,azyx,bzyx->abzyx", rho, u, u).reshape(9, nz, ny, nx)).reshape(3, 3, cz, cy, cx)
     tau = uu / 8.0 - rb * np.einsum("azyx,bzyx->abzyx", ub, ub)
+    # each fine cell's viscous stress from its post-collision stress
+    m2 = np.einsum("ia,ib,izyx->abzyx", e, e, f)
+    pst = m2 - rho / 3.0 * np.eye(3)[:, :, None, None, None] - np.einsum("zyx,azyx,bzyx->abzyx", rho, u, u)
+    pmag = np.sqrt((pst * pst).sum(axis=(0, 1)))
+    kq = 18.0 * 1.41421356 * cs_f * cs_f
+    disc = np.maximum((1.0 - tau_f) ** 2 - kq * pmag / np.maximum(rho, 1e-6), 0.0)
+    te = 0.5 * ((1.0 + tau_f) - np.sqrt(disc))
+    vf = (te - 0.5) / (1.0 - te) * pst
+    vis = blk(vf.reshape(9, nz, ny, nx)).reshape(3, 3, cz, cy, cx) / 8.0
     rows = []
     for z in range(1, cz - 1):
         for y in range(1, cy - 1):
@@ -81,12 +93,12 @@ def _box_filter_samples(pops, solid, tau_c, filter_width):
                 g = np.stack([gx, gy, gz])
                 s = 0.5 * (g + g.T)
                 sd = s - np.trace(s) / 3 * np.eye(3)
-                t = tau[:, :, z, y, x]
+                t = vis[:, :, z, y, x] - tau[:, :, z, y, x]
                 td = t - np.trace(t) / 3 * np.eye(3)
                 sds = (sd * sd).sum()
                 if not sds > 1e-18:
                     continue
-                nu = max(0.0, -(td * sd).sum() / (2 * rb[z, y, x] * sds))
+                nu = max(0.0, (td * sd).sum() / (2 * rb[z, y, x] * sds) - (tau_c - 0.5) / 3.0)
                 p = -(2.0 / 3.0) * rb[z, y, x] * (tau_c + 3 * nu) * s
                 mag = np.sqrt((p * p).sum())
                 rows.append([np.log2(mag / rb[z, y, x] + 1e-12), np.trace(p) / mag, np.linalg.det(p) / mag ** 3,
@@ -104,7 +116,7 @@ def test_closure_samples_match_numpy(gpu, oracle_built):
     s.Reset(Params(tau=0.52, inletVelocity=0.08, smagorinskyCs=0.1), True)
     s.Step(None, 150)
     rows = s.ClosureSamples(2.0).cpu().numpy()
-    want = _box_filter_samples(s.SavePopulations(), solid, 0.5 + 0.5 * (0.52 - 0.5), 2.0)
+    want = _box_filter_samples(s.SavePopulations(), solid, 0.5 + 0.5 * (0.52 - 0.5), 2.0, 0.52, 0.1)
     assert len(rows) == len(want) > 200
     assert np.isfinite(rows).all() and (rows[:, 5] >= 0).all()
     for k in (0, 5):

@@ -49,13 +49,16 @@ class FakeSolver:
                 acc = acc * 0.5 + f[(d + 2) % 3, z + d]
         return acc
 
-    def LayerCopy(self, z, buf, to_buffer, next_set=False, cmd=None):
+    def LayerCopy(self, z, buf, to_buffer, next_set=False, cmd=None, ez=0):
+        """ez = +1 / -1: only the population moving in +z / -z, as the
+        buffer's first row (the stand-in's one plane per direction)."""
         p = self.pop[1 - self.cur if next_set else self.cur]
         b = buf.tensor.numpy()
+        planes = [1] if ez == 1 else ([2] if ez == -1 else [0, 1, 2])
         if to_buffer:
-            b[...] = p[:, z]
+            b[:len(planes)] = p[planes, z]
         else:
-            p[:, z] = b
+            p[planes, z] = b[:len(planes)]
 
 
 class HostBuffer:
@@ -86,7 +89,7 @@ def slab_stepper(init, rank, world, exchange):
     lay = shard.layout(init.shape[1], rank, world)
     s = FakeSolver(init[:, lay.lo:lay.hi])
     bufs = tuple(HostBuffer(3, init.shape[2]) for _ in range(4))
-    return s, lay, shard.SlabStepper(s, lay, bufs, exchange, rank)
+    return s, lay, shard.SlabStepper(s, lay, bufs, exchange, rank, dir_rows=1)
 
 
 def test_slab_ranges_cover_and_balance():
@@ -129,6 +132,18 @@ def test_split_matches_unsplit(nz, world):
     shard.refresh_emulated([st for _, _, st in ranks])
     for s, lay, _ in ranks:
         np.testing.assert_array_equal(owned_readback(s, lay), rb[lay.z0:lay.z1])
+
+
+def test_step_exchange_moves_only_the_streaming_planes():
+    """Per step a side sends the planes streaming across the cut (one of the
+    stand-in's three, 5 of D3Q19's 19); refresh sends whole layers."""
+    init = initial(8)
+    _, _, st = slab_stepper(init, 0, 2, None)
+    (peer, send, recv), = st.posts(st.dir_rows)
+    assert peer == 1 and send.tensor.shape[0] == 1 and recv.tensor.shape[0] == 1
+    (_, send, _), = st.posts()
+    assert send.tensor.shape[0] == 3
+    assert shard.DIR_PLANES == 5
 
 
 def test_stale_outer_halo_is_detected():
