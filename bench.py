@@ -99,6 +99,8 @@ def parse_args(argv=None):
                          "device copies as the exchange")
     ap.add_argument("--shard-ranks", type=int, default=2, help="slabs emulated on one GPU with --shard at N=1")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--batch-steps", type=int, default=200,
+                    help="steps of the 16-lattice sweep set (C3) timed after the default run's variants; 0 skips")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     return ap.parse_args(argv)
@@ -470,14 +472,13 @@ def run_e2e(args, cfg, solid, sdf, variant, dev_index):
                      "steps for the learned variants"}
 
 
-def run_batch(args, cfg, rank, world, local_rank):
-    """The c3 set: every rank steps its own batch of 16 lattices."""
+def time_batch(args, cfg, local_rank, dist_on, steps, sample_clocks):
+    """The c3 set stepped as one batch (autotuned), timed with events; and the
+    same lattices stepped one after another for contrast."""
     import torch
 
     from flowcraft_b200.batch import LbmBatch
     from flowcraft_b200.sweep import c3_lattices, make_members
-    dist_on = world > 1
-    torch.cuda.set_device(local_rank)
     mem = make_members(c3_lattices(), "FP16_OFFSET", cfg["cs"], local_rank)
     solvers = [m[0] for m in mem]
     cells = sum(s.CellCount() for s in solvers)
@@ -491,8 +492,8 @@ def run_batch(args, cfg, rank, world, local_rank):
     b.Step(2 * args.warmup)
     torch.cuda.synchronize()
     barrier_sync(dist_on)
-    sampler = ClockSampler(local_rank) if rank == 0 else None
-    steps = args.steps + (args.steps & 1)
+    sampler = ClockSampler(local_rank) if sample_clocks else None
+    steps = steps + (steps & 1)
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
     # the batch runs on its own stream, ordered after and before the members'
@@ -517,18 +518,32 @@ def run_batch(args, cfg, rank, world, local_rank):
     seq_ms = seq_start.elapsed_time(seq_stop)
     barrier_sync(dist_on)
     ms = allreduce_max(ms, dist_on)
-    diverged = [s.HasDiverged() for s in solvers]
+    diverged = any(s.HasDiverged() for s in solvers)
+    bulk_cells = sum(s.BoundaryInfo()["bulk_cells"] for s in solvers)
     b.close()
+    for s in solvers:
+        s.close()
+    return dict(cells=cells, bulk_cells=bulk_cells, steps=steps, ms=ms, seq_ms=seq_ms, tuned=tuned, clocks=clocks,
+                diverged=diverged, sizes=[m[1]["nx"] for m in mem], lattices=len(solvers))
+
+
+def run_batch(args, cfg, rank, world, local_rank):
+    """The c3 set: every rank steps its own batch of 16 lattices."""
+    import torch
+    dist_on = world > 1
+    torch.cuda.set_device(local_rank)
+    r = time_batch(args, cfg, local_rank, dist_on, args.steps, rank == 0)
     if rank != 0:
         return 0
+    cells, steps, ms, seq_ms, tuned, clocks = r["cells"], r["steps"], r["ms"], r["seq_ms"], r["tuned"], r["clocks"]
     value = world * cells * steps / (ms / 1e3) / 1e9
     line = {"metric": METRIC, "value": value, "unit": "GLUPS", "n_gpus": world, "steps": steps,
             "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic: analytic NACA 2412 lattices on the device",
-            "config": {"workload": cfg["desc"], "lattices": len(solvers), "cells": cells,
-                       "sizes": [m[1]["nx"] for m in mem], "autotune": tuned,
+            "config": {"workload": cfg["desc"], "lattices": r["lattices"], "cells": cells,
+                       "sizes": r["sizes"], "autotune": tuned,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-            "diverged": any(diverged), "gpu_launches": (2 if tuned["rows"] else len(solvers) + 1) * steps,
+            "diverged": r["diverged"], "gpu_launches": (2 if tuned["rows"] else r["lattices"] + 1) * steps,
             "clocks": clocks,
             "sequential": {"glups": world * cells * steps / (seq_ms / 1e3) / 1e9, "ms_per_step": seq_ms / steps,
                            "how": "the same lattices stepped one after another on one stream with LbmSolver.Step"}}
@@ -658,6 +673,19 @@ def run_ours(args, cfg, rank, world, local_rank):
                         else f"fallback: {FALLBACK_HBM_GBS:.0f} GB/s, an earlier copy measurement on this GPU type "
                              "(no MEASURED_PEAKS.json)"),
     }
+    # the batched sweep set (C3), compact, so the default run records it too
+    batch_c3 = None
+    if args.config == "large" and args.batch_steps > 0:
+        del solid, sdf
+        torch.cuda.empty_cache()
+        r = time_batch(args, CONFIGS["c3"], local_rank, dist_on, args.batch_steps, False)
+        bg = world * r["cells"] * r["steps"] / (r["ms"] / 1e3) / 1e9
+        bb = r["bulk_cells"] * 76 * r["steps"] / (r["ms"] / 1e3) / 1e9  # FP16 bytes per bulk cell update
+        shape = "per_member" if r["tuned"]["rows"] == 0 else f"rows{r['tuned']['rows']}_x{r['tuned']['grid_mult']}"
+        batch_c3 = {"glups": round(bg, 2), "frac": round(bb / peak, 3), "shape": shape, "steps": r["steps"],
+                    "sequential_glups": round(world * r["cells"] * r["steps"] / (r["seq_ms"] / 1e3) / 1e9, 2),
+                    "cells": r["cells"], "diverged": r["diverged"]}
+        solid, sdf = build_geometry(cfg, f"cuda:{local_rank}")
     e2e = None
     if not args.no_e2e:
         torch.cuda.empty_cache()
@@ -703,6 +731,7 @@ def run_ours(args, cfg, rank, world, local_rank):
                    "boundary_cells": head["boundary_cells"], "bouzidi_links": head["bouzidi_links"],
                    "closure_coverage": head["closure_coverage"]},
         "variants": variants_out,
+        "batch_c3": batch_c3,
         "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": e2e,

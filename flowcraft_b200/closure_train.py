@@ -279,6 +279,8 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--max-samples", type=int, default=10_000_000)
+    ap.add_argument("--wall-min", type=float, default=8.0,
+                    help="cells nearer a wall than this keep Smagorinsky when the closure runs (stored in the file)")
     ap.add_argument("--out", required=True)
     args = ap.parse_args(argv)
     import time
@@ -294,6 +296,7 @@ def main(argv=None):
         samples, tau_c = samples[keep], tau_c[keep.cpu().numpy()]
     t1 = time.time()
     cw, rep = train_closure(samples, tau_c, epochs=args.epochs, batch=args.batch, lr=args.lr)
+    cw.wall_min = args.wall_min
     t2 = time.time()
     cw.meta.update({"fine_lattice": [512 // args.scale, 256 // args.scale, 256 // args.scale],
                     "sample_seconds": round(t1 - t0, 1), "train_seconds": round(t2 - t1, 1),

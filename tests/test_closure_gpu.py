@@ -226,3 +226,54 @@ def test_fallback_reproduces_smagorinsky(gpu):
         a.step(5)
         b.step(5)
         assert np.abs(a.readback_field().astype(np.float64) - b.readback_field()).max() < 4 * tol
+
+
+@pytest.mark.parametrize("wall_min,trust", [(2.0, 0.0), (0.0, 1.5), (1.5, 2.0)])
+def test_near_wall_fallback_and_anchoring_vs_fp64_oracle(gpu, oracle_built, wall_min, trust):
+    """The closure's near-wall Smagorinsky fallback (cells nearer a wall than
+    wall_min cells) and its Smagorinsky trust band (3 nu_t within a factor
+    `trust`): 40 FP16 steps against the FP64 oracle running the same rules;
+    the probe leaves the near-wall cells out of the covered set; and the same
+    rules under in-place AA streaming give the ping-pong result bit for bit."""
+    from flowcraft_b200.lbm import LatticeModel, LbmSolver, Params, Storage, Streaming, VoxelGrid
+    case = _shape_case(*SHAPES[0][1:], q=19)
+    probe = GpuAdapter(case, storage=Storage.FP16_OFFSET)
+    probe.step(30)
+    cw = _weights(probe)
+    cw.wall_min, cw.trust = wall_min, trust
+    probe.s.SetClosure(cw)
+    x, _, in_range = probe.s.ClosureProbe()
+    near = x[:, 3] < wall_min
+    assert not in_range[near].any()
+    if wall_min > 0:
+        assert near[~probe.solid.ravel().astype(bool)].sum() > 0
+    probe.s.close()
+    sim = GpuAdapter(case, storage=Storage.FP16_OFFSET)
+    sim.s.SetClosure(cw)
+    ref = OracleAdapter(case, "f64")
+    ref.o.set_closure(cw)
+    sim.step(40)
+    ref.step(40)
+    g = sim.readback_field().reshape(-1, 4).astype(np.float64)
+    r = ref.o.readback_field_f64().reshape(-1, 4)
+    solid = geometry(case["geom"])[0].ravel().astype(bool)
+    d = np.abs(g - r)[~solid]
+    print(f"wall_min {wall_min} trust {trust}: max|drho| {d[:, 0].max():.3e} max|du| {d[:, 1:].max():.3e}")
+    assert np.isfinite(g).all()
+    assert d[:, 0].max() < 3e-4 and d[:, 1:].max() < 3e-4
+    # in place: bit-identical populations
+    s, sdf_solid = geometry(case["geom"])
+    nz, ny, nx = s.shape
+    p = case["params"]
+    prm = Params(tau=p["tau"], inletVelocity=p["inlet_velocity"], reverseFlow=bool(p.get("reverse_flow", 0)),
+                 freeSlipY=bool(p.get("free_slip_y", 1)), freeSlipZ=bool(p.get("free_slip_z", 1)),
+                 smagorinskyCs=p["smagorinsky_cs"])
+    aa = LbmSolver()
+    assert aa.Init(0, VoxelGrid(nx, ny, nz, solid=s, signedDistance=sdf_solid), LatticeModel.D3Q19,
+                   Storage.FP16_OFFSET, Streaming.AA), aa.LastError()
+    aa.Reset(prm, case["seed_mid"])
+    aa.SetClosure(cw)
+    aa.Step(None, 40)
+    assert np.array_equal(aa.SavePopulations(), sim.s.SavePopulations())
+    aa.close()
+    sim.s.close()
