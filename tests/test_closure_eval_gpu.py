@@ -7,6 +7,10 @@ the forces.
   smaller time-averaged wake velocity error than the coarse run with
   Smagorinsky, and its drag error is no more than one percentage point
   worse.
+* On the precision configuration's NACA 0012 wing at full size (384x192x192,
+  Re 1e4, 5000 steps, forces averaged over the last fifth): FP16 storage with
+  the learned closure keeps the drag and lift within 1 % of the FP32
+  Smagorinsky run, the north star's bound.
 * On the large configuration's aircraft at half size (512x256x256, the mesh
   voxelized on the device, Re 1e5 on the 30-cell root chord, 1500 steps,
   forces averaged over the last fifth): FP16 storage with Smagorinsky stays
@@ -42,12 +46,12 @@ def test_learned_closure_closer_to_filtered_fine_run(gpu, name):
     assert abs(l["drag_vs_fine"]) < abs(s["drag_vs_fine"]) + 0.01
 
 
-def _avg_forces(solid, sdf, storage, closure, tau, steps=1500):
+def _avg_forces(solid, sdf, storage, closure, tau, steps=1500, u=0.05):
     from flowcraft_b200.lbm import LatticeModel, LbmSolver, Params, Storage, VoxelGrid
     nz, ny, nx = solid.shape
     s = LbmSolver()
     assert s.Init(0, VoxelGrid(nx, ny, nz, solid=solid, signedDistance=sdf), LatticeModel.D3Q19, Storage[storage])
-    s.Reset(Params(tau=tau, inletVelocity=0.05, smagorinskyCs=0.1), True)
+    s.Reset(Params(tau=tau, inletVelocity=u, smagorinskyCs=0.1), True)
     if closure is not None:
         s.SetClosure(closure)
     a0 = steps - steps // 5
@@ -60,6 +64,21 @@ def _avg_forces(solid, sdf, storage, closure, tau, steps=1500):
     assert not s.HasDiverged()
     s.close()
     return acc / n
+
+
+def test_learned_closure_within_1pct_on_the_precision_wing(gpu):
+    import sys
+
+    sys.path.insert(0, __import__("os").path.dirname(__file__))
+    import precision_study as ps
+    c = ps.case(False)
+    solid, sdf = ps.geometry(c)
+    tau = ps.tau_of(c)
+    ref = _avg_forces(solid, sdf, "FP32", None, tau, steps=c["steps"], u=ps.U)
+    learned = _avg_forces(solid, sdf, "FP16_OFFSET", _shipped(), tau, steps=c["steps"], u=ps.U)
+    dcd, dcl = learned[0] / ref[0] - 1.0, learned[2] / ref[2] - 1.0
+    print("precision wing: FP16 learned dCd %+.4f dCl %+.4f against FP32 Smagorinsky" % (dcd, dcl))
+    assert abs(dcd) < 0.01 and abs(dcl) < 0.01
 
 
 def test_aircraft_forces_envelope(gpu):
