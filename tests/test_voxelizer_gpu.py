@@ -92,7 +92,8 @@ def test_empty_and_invalid_meshes(gpu):
 
 def test_voxelized_c1_obstacle_steps_bit_exact(gpu, oracle_built):
     """Mesh -> device voxel grid -> solver, against the oracle solver on the
-    oracle's voxelization of the same mesh (the c1 obstacle, 128x64x64)."""
+    oracle's voxelization of the same mesh (the c1 obstacle, 128x64x64), for
+    the configuration's 1000 steps."""
     import torch
     from flowcraft_b200.lbm import LatticeModel, LbmSolver, Params
     from flowcraft_b200.voxelizer import VoxelizeOnGrid
@@ -106,11 +107,11 @@ def test_voxelized_c1_obstacle_steps_bit_exact(gpu, oracle_built):
     s = LbmSolver()
     assert s.Init(0, g, LatticeModel.D3Q19), s.LastError()
     s.Reset(params)
-    s.Step(None, 100)
+    s.Step(None, 1000)
     got = s.ReadbackField()
     s.close()
     o = oracle_built.Oracle(want_s, want_d, 19, oracle_built.Params(params.tau, 0.05, False, True, True, 0.1))
-    o.step(100)
+    o.step(1000)
     want = o.readback_field()
     o.close()
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
