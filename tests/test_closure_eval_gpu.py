@@ -10,14 +10,13 @@ the forces.
 * On the precision configuration's NACA 0012 wing at full size (384x192x192,
   Re 1e4, 5000 steps, forces averaged over the last fifth): FP16 storage with
   the learned closure keeps the drag and lift within 1 % of the FP32
-  Smagorinsky run, the north star's bound.
+  Smagorinsky run, the accuracy bound the benchmark's pairing states.
 * On the large configuration's aircraft at half size (512x256x256, the mesh
   voxelized on the device, Re 1e5 on the 30-cell root chord, 1500 steps,
   forces averaged over the last fifth): FP16 storage with Smagorinsky stays
   within 2 % of FP32 Smagorinsky in drag and lift, and FP16 with the learned
-  closure within 5 %. The north star's 1 % for the learned closure is not
-  met on this case; FP16 storage alone already moves drag by about 1 %
-  here."""
+  closure within 5 %. The 1 % bound for the learned closure is not met on
+  this case; FP16 storage alone already moves drag by about 1 % here."""
 import numpy as np
 import pytest
 
