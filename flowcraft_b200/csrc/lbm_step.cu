@@ -142,6 +142,66 @@ __device__ __forceinline__ void plane_cell(const typename S::T* __restrict__ fin
     });
 }
 
+// The inlet / outlet cells a warp of the pair kernels holds, updated by the
+// whole warp for the 16-bit formats: lane i < Q takes population i, so a
+// cell's Q loads and Q stores are one instruction each for the warp instead
+// of Q for one lane while the other lanes wait. The values, the moments
+// (direction order, shared by shuffles) and the equilibrium are those of
+// plane_cell. Every lane of the warp calls row_end_cells together; `plane`
+// holds this lane's bits (1: cell x, 2: cell x + 1). (The FP32 kernels keep
+// plane_cell: there the warp-wide version costs more registers than the
+// kernel has to spare.)
+template <int Q>
+__device__ __forceinline__ float lattice_w_rt(unsigned i) {
+    return i == 0 ? Lattice<Q>::w(0) : (i < 7 ? Lattice<Q>::w(1) : Lattice<Q>::w(Q - 1));
+}
+
+template <int Q, class S>
+__device__ __forceinline__ void row_end_cell(const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
+                                             const Geom& g, const StepParams& p, int px, size_t pc) {
+    const unsigned lane = threadIdx.x & 31;
+    const bool mine = lane < (unsigned)Q;
+    const unsigned i = mine ? lane : 0u;
+    const float wi = lattice_w_rt<Q>(i);
+    typename S::T* dst = fout + (size_t)i * g.n + pc;
+    if (px == p.inlet_x) {
+        float v = p.feq_inlet[0];
+        static_for<1, Q>([&](auto I) {
+            if (i == decltype(I)::value) v = p.feq_inlet[decltype(I)::value];
+        });
+        if (mine) *dst = S::enc(v, wi);
+        return;
+    }
+    const size_t nb = p.reverse ? pc + 1 : pc - 1;
+    const float own = S::dec(S::ld(fin + (size_t)i * g.n + nb), wi);
+    float f[Q];
+    static_for<0, Q>([&](auto I) { f[decltype(I)::value] = __shfl_sync(0xffffffffu, own, decltype(I)::value); });
+    float nr, nu, nv, nw;
+    moments<Q>(f, nr, nu, nv, nw);
+    const float rho = nr > 1e-6f ? 1.0f + 0.999f * (nr - 1.0f) : 1.0f;
+    equilibrium_all<Q>(rho, nu, nv, nw, f);
+    float o = f[0];
+    static_for<1, Q>([&](auto I) {
+        if (i == decltype(I)::value) o = f[decltype(I)::value];
+    });
+    if (mine) *dst = S::enc(o, wi);
+}
+
+template <int Q, class S>
+__device__ __forceinline__ void row_end_cells(const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
+                                              const Geom& g, const StepParams& p, unsigned plane, int x, uint32_t c) {
+    unsigned m = __ballot_sync(0xffffffffu, plane != 0u);
+    while (m) {  // uniform: at most the two row ends
+        const int src = __ffs(m) - 1;
+        m &= m - 1u;
+        const unsigned sp = __shfl_sync(0xffffffffu, plane, src);
+        const int sx = __shfl_sync(0xffffffffu, x, src);
+        const uint32_t sc = __shfl_sync(0xffffffffu, c, src);
+        if (sp & 1u) row_end_cell<Q, S>(fin, fout, g, p, sx, (size_t)sc);
+        if (sp & 2u) row_end_cell<Q, S>(fin, fout, g, p, sx + 1, (size_t)sc + 1);
+    }
+}
+
 // Bulk cells of lattices with even nx, two x-adjacent cells per thread, every
 // row and every 64-cell chunk. A warp covers cells [64*blockIdx.x, +64) of one
 // row, so whether it touches a Y/Z domain face (`face`) or the first or last
@@ -253,13 +313,17 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs(const typename
         plane |= pair & 2u;
         pair &= ~2u;
     }
-    if (!(pair | plane)) return;
     const uint32_t c = (uint32_t)(row * g.nx + x);
+    if constexpr (!S::kExact) {  // the row-end cells by the whole warp (no interior warp holds one)
+        row_end_cells<Q, S>(fin, fout, g, p, plane, x, c);
+        plane = 0;
+    }
+    if (!(pair | plane)) return;
     const bool face = (y == 0) | (y == g.ny - 1) | (z == 0) | (z == g.nz - 1);
     const bool edge = (bx == 0) | (64 * bx + 64 >= g.nx);
     if (sh.n && !face && !edge) return;  // an interior warp: done by k_bulk_tiles
 
-    // the one lane of a row end that holds an inlet or outlet cell finishes it alone
+    // FP32: the one lane of a row end that holds an inlet or outlet cell finishes it alone
     if (plane) plane_cell<Q, S>(fin, fout, g, p, plane == 1u ? x : x + 1, plane == 1u ? c : (size_t)c + 1);
     if (!pair) return;
     float2 v[Q];
@@ -352,7 +416,7 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned(const 
     }
     const uint32_t c = (uint32_t)(row * g.nx + x);
     const bool face = (y == 0) | (y == g.ny - 1) | (z == 0) | (z == g.nz - 1);
-    if (plane) plane_cell<Q, S>(fin, fout, g, p, plane == 1u ? x : x + 1, plane == 1u ? c : (size_t)c + 1);
+    row_end_cells<Q, S>(fin, fout, g, p, plane, x, c);
     const bool va = pair & 1u, vb = pair & 2u;
 
     // The load path is chosen per warp: off the Y/Z faces every lane takes
@@ -493,7 +557,7 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_learned_tc(con
     }
     const uint32_t c = (uint32_t)(row * g.nx + x);
     const bool face = (y == 0) | (y == g.ny - 1) | (z == 0) | (z == g.nz - 1);
-    if (plane) plane_cell<Q, S>(fin, fout, g, p, plane == 1u ? x : x + 1, plane == 1u ? c : (size_t)c + 1);
+    row_end_cells<Q, S>(fin, fout, g, p, plane, x, c);
     const bool va = pair & 1u, vb = pair & 2u;
 
     // The load path is chosen per warp: off the Y/Z faces every lane takes
