@@ -156,6 +156,34 @@ __device__ __forceinline__ float lattice_w_rt(unsigned i) {
     return i == 0 ? Lattice<Q>::w(0) : (i < 7 ? Lattice<Q>::w(1) : Lattice<Q>::w(Q - 1));
 }
 
+// Component `axis` of e_i for a run-time direction: the table packed two bits
+// per direction (component + 1) into one compile-time constant.
+template <int Q>
+__host__ __device__ constexpr unsigned long long lattice_e_bits(int axis) {
+    unsigned long long b = 0;
+    for (int i = 0; i < Q; ++i) {
+        const int e = axis == 0 ? Lattice<Q>::ex(i) : (axis == 1 ? Lattice<Q>::ey(i) : Lattice<Q>::ez(i));
+        b |= (unsigned long long)(e + 1) << (2 * i);
+    }
+    return b;
+}
+
+template <int Q, int Axis>
+__device__ __forceinline__ float lattice_e_rt(unsigned i) {
+    constexpr unsigned long long bits = lattice_e_bits<Q>(Axis);
+    return (float)((int)((bits >> (2 * i)) & 3ull) - 1);
+}
+
+// equilibrium<Q, I> for a run-time direction: e.u as ((ex ux + ey uy) + ez uz)
+// with e in {-1, 0, 1}, which equals edotu's sum of the non-zero terms (a
+// zero term adds +-0, and only the sign of a zero result can differ, which
+// the equilibrium does not see), then the same operations.
+template <int Q>
+__device__ __forceinline__ float equilibrium_rt(unsigned i, float rho, float ux, float uy, float uz, float u2) {
+    const float eu = (lattice_e_rt<Q, 0>(i) * ux + lattice_e_rt<Q, 1>(i) * uy) + lattice_e_rt<Q, 2>(i) * uz;
+    return (lattice_w_rt<Q>(i) * rho) * (((1.0f + 3.0f * eu) + (4.5f * eu) * eu) - 1.5f * u2);
+}
+
 template <int Q, class S>
 __device__ __forceinline__ void row_end_cell(const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
                                              const Geom& g, const StepParams& p, int px, size_t pc) {
@@ -164,11 +192,9 @@ __device__ __forceinline__ void row_end_cell(const typename S::T* __restrict__ f
     const unsigned i = mine ? lane : 0u;
     const float wi = lattice_w_rt<Q>(i);
     typename S::T* dst = fout + (size_t)i * g.n + pc;
-    if (px == p.inlet_x) {
-        float v = p.feq_inlet[0];
-        static_for<1, Q>([&](auto I) {
-            if (i == decltype(I)::value) v = p.feq_inlet[decltype(I)::value];
-        });
+    if (px == p.inlet_x) {  // feq_inlet[i]: the equilibrium at rho 1, u = (inlet_ux, 0, 0)
+        const float ux = p.inlet_ux;
+        const float v = equilibrium_rt<Q>(i, 1.0f, ux, 0.0f, 0.0f, speed2(ux, 0.0f, 0.0f));
         if (mine) *dst = S::enc(v, wi);
         return;
     }
@@ -179,11 +205,7 @@ __device__ __forceinline__ void row_end_cell(const typename S::T* __restrict__ f
     float nr, nu, nv, nw;
     moments<Q>(f, nr, nu, nv, nw);
     const float rho = nr > 1e-6f ? 1.0f + 0.999f * (nr - 1.0f) : 1.0f;
-    equilibrium_all<Q>(rho, nu, nv, nw, f);
-    float o = f[0];
-    static_for<1, Q>([&](auto I) {
-        if (i == decltype(I)::value) o = f[decltype(I)::value];
-    });
+    const float o = equilibrium_rt<Q>(i, rho, nu, nv, nw, speed2(nu, nv, nw));
     if (mine) *dst = S::enc(o, wi);
 }
 
@@ -237,12 +259,12 @@ __device__ __forceinline__ void store_pair(const PlanePtrs& pp, uint32_t c, cons
             T* dst = static_cast<T*>(pp.dst[decltype(I)::value]);
             *reinterpret_cast<typename S::T2*>(dst + c) = enc(I);
         });
-    } else {
+    } else {  // one cell of the pair (pair is 1 or 2): one element store per plane
+        const uint32_t ec = pair == 1u ? c : c + 1u;
         static_for<0, Q>([&](auto I) {
             T* dst = static_cast<T*>(pp.dst[decltype(I)::value]);
             const typename S::T2 h = enc(I);
-            if (pair & 1u) dst[c] = h.x;
-            if (pair & 2u) dst[c + 1u] = h.y;
+            dst[ec] = pair == 1u ? h.x : h.y;
         });
     }
 }
