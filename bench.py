@@ -62,8 +62,9 @@ CONFIGS = {
     "c3": dict(nx=0, ny=0, nz=0, geom="batch", u=0.0, re=0.0, lref=0.0, cs=0.1,
                desc="D3Q19 batch of 16 NACA 2412 wing lattices, sizes 64x32x32..256x128x128 (2:1:1) drawn with seed "
                     "20261203, chord 0.375 nx, AoA -8..14 deg, U 0.04-0.08, Re 1e3-2e4, FP16 offset, Smagorinsky "
-                    "Cs=0.1, all lattices stepped as one batch per step in a CUDA graph (autotuned: one persistent "
-                    "launch, or the lattices' own bulk kernels side by side)"),
+                    "Cs=0.1, all lattices stepped as one batch per step in a CUDA graph (autotuned: one launch over "
+                    "every lattice's tiles, persistent or one block per tile, or the lattices' own bulk kernels "
+                    "side by side)"),
     # the precision-study lattice size: 384x192x192 NACA 0012 wing, chord 96, 4 deg
     "c2": dict(nx=384, ny=192, nz=192, geom="naca0012", u=0.06, re=1e4, lref=96.0, cs=0.1,
                desc="D3Q19 384x192x192 (14.2M cells), NACA 0012 wing chord 96 span 128 at 4 deg, U=0.06, "
@@ -92,7 +93,8 @@ def parse_args(argv=None):
     ap.add_argument("--spinup", type=int, default=2000,
                     help="untimed steps from the seed before the warm-up of the learned variants (flow state)")
     ap.add_argument("--batch-shape", default=None,
-                    help="c3 only: ROWSxMULT (e.g. 4x2, or 0x1 for per-member launches) instead of the autotuner")
+                    help="c3 only: ROWSxMULT (e.g. 4x2; 8x0 for one block per tile; 0x1 for per-member launches) "
+                         "instead of the autotuner")
     ap.add_argument("--shard", action="store_true",
                     help="one lattice split into z-slabs across the ranks (NCCL point-to-point halo exchange), "
                          "FP16 offset storage with Smagorinsky; on one GPU, --shard-ranks slabs emulated with "
@@ -681,7 +683,8 @@ def run_ours(args, cfg, rank, world, local_rank):
         r = time_batch(args, CONFIGS["c3"], local_rank, dist_on, args.batch_steps, False)
         bg = world * r["cells"] * r["steps"] / (r["ms"] / 1e3) / 1e9
         bb = r["bulk_cells"] * 76 * r["steps"] / (r["ms"] / 1e3) / 1e9  # FP16 bytes per bulk cell update
-        shape = "per_member" if r["tuned"]["rows"] == 0 else f"rows{r['tuned']['rows']}_x{r['tuned']['grid_mult']}"
+        from flowcraft_b200.batch import candidate_name
+        shape = candidate_name((r["tuned"]["rows"], r["tuned"]["grid_mult"]))
         batch_c3 = {"glups": round(bg, 2), "frac": round(bb / peak, 3), "shape": shape, "steps": r["steps"],
                     "sequential_glups": round(world * r["cells"] * r["steps"] / (r["seq_ms"] / 1e3) / 1e9, 2),
                     "cells": r["cells"], "diverged": r["diverged"]}

@@ -1,7 +1,7 @@
 """Many lattices stepped together (``fc_lbm_batch_*`` in include/fc_lbm.h):
-one persistent bulk launch over the tiles of every member per step (or each
-member's own bulk kernel, side by side, when the autotuner finds that
-faster), pairs of steps replayed as a CUDA graph, block shape picked by an
+one bulk launch over the tiles of every member per step (persistent, or one
+block per tile; or each member's own bulk kernel, side by side, when the
+autotuner finds that faster), pairs of steps replayed as a CUDA graph, block shape picked by an
 autotuner. The
 members stay ordinary ``LbmSolver`` objects (readbacks, forces, SetParams);
 the batch only steps them, bit-identically to ``LbmSolver.Step``."""
@@ -13,9 +13,16 @@ import numpy as np
 
 from .lbm import FC_LBM_OK, LbmError, load_library
 
-# the persistent launch's block shapes, then rows 0: every member's own bulk
-# kernel, run side by side on forked streams
-CANDIDATES = [(r, m) for r in (4, 8, 16) for m in (1, 2)] + [(0, 1)]
+# (rows, grid_mult): the persistent launch's block shapes (grid_mult 1, 2),
+# the one-block-per-tile launch (8, 0), then rows 0: every member's
+# own bulk kernel, run side by side on forked streams
+CANDIDATES = [(r, m) for r in (4, 8, 16) for m in (1, 2)] + [(8, 0), (0, 1)]
+
+
+def candidate_name(c) -> str:
+    if not c[0]:
+        return "per_member"
+    return "per_tile" if c[1] == 0 else f"rows{c[0]}_x{c[1]}"
 
 
 class LbmBatch:
@@ -49,7 +56,7 @@ class LbmBatch:
         self._check(self._lib.fc_lbm_batch_tune(self._h, int(steps), ctypes.byref(r), ctypes.byref(m), ms),
                     "batch tune")
         return {"rows": r.value, "grid_mult": m.value,
-                "ms_per_step": {(f"rows{c[0]}_x{c[1]}" if c[0] else "per_member"): float(ms[i])
+                "ms_per_step": {candidate_name(c): float(ms[i])
                                 for i, c in enumerate(CANDIDATES)}}
 
     def close(self):

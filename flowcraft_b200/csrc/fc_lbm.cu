@@ -1388,6 +1388,8 @@ struct fc_lbm_batch {
     cudaEvent_t ev = nullptr;
     fc::BatchLattice* d_lat = nullptr;
     std::vector<fc::BatchLattice> h_lat;
+    // grid_mult 0: the one-block-per-tile launches of each step parity
+    std::vector<fc::TileLaunch> tiles[2];
     unsigned long long total = 0;   // bulk work items
     unsigned long long btotal = 0;  // boundary-list entries
     int rows = 8, mult = 1, grid = 0;  // rows 0: every member's own bulk launch
@@ -1403,8 +1405,10 @@ struct fc_lbm_batch {
 namespace {
 
 // The autotuner's candidates, in the order of fc_lbm_batch_tune's times: the
-// persistent launch's block shapes, then every member's own bulk kernel.
-constexpr int kBatchCand[FC_LBM_BATCH_CANDIDATES][2] = {{4, 1}, {4, 2}, {8, 1}, {8, 2}, {16, 1}, {16, 2}, {0, 1}};
+// persistent launch's block shapes, the one-block-per-tile launch, then every
+// member's own bulk kernel.
+constexpr int kBatchCand[FC_LBM_BATCH_CANDIDATES][2] = {{4, 1}, {4, 2}, {8, 1}, {8, 2}, {16, 1}, {16, 2},
+                                                      {8, 0}, {0, 1}};
 
 int bfail(fc_lbm_batch* b, int code, const std::string& msg) {
     b->err = msg;
@@ -1483,11 +1487,39 @@ int batch_build(fc_lbm_batch* b) {
     }
     b->total = first;
     b->btotal = bfirst;
+    for (int par = 0; par < 2; ++par) {  // one block per tile: up to 32 lattices per launch
+        b->tiles[par].clear();
+        if (!b->rows || b->mult != 0) continue;
+        for (size_t k = 0; k < b->m.size(); ++k) {
+            const fc::BatchLattice& d = b->h_lat[k];
+            const unsigned long long n = (unsigned long long)d.gx * d.gy * d.g.nz;
+            if (b->tiles[par].empty() || b->tiles[par].back().nlat == fc::kTileLaunchLattices ||
+                b->tiles[par].back().tiles + n > 0x7fffffffull) {
+                if (n > 0x7fffffffull) return bfail(b, FC_LBM_ERR_UNSUPPORTED, "one block per tile: 2^31 tiles at most");
+                b->tiles[par].emplace_back();
+                std::memset(&b->tiles[par].back(), 0, sizeof(fc::TileLaunch));
+            }
+            fc::TileLaunch& t = b->tiles[par].back();
+            fc::TileLattice& l = t.l[t.nlat++];
+            const int side = d.cur ^ par;
+            l.g = d.g;
+            l.p = d.p;
+            l.pp = d.pp[side];
+            l.fin = d.pop[side];
+            l.fout = const_cast<void*>(d.pop[side ^ 1]);
+            l.bits = d.bits;
+            l.diverged = d.diverged;
+            l.first = t.tiles;
+            l.gx = d.gx;
+            l.gy = d.gy;
+            t.tiles += (unsigned)n;
+        }
+    }
     const int resident = fc::bulk_batch_resident(b->q, b->storage, b->rows ? b->rows : 8);
     int sms = 0;
     FB_TRY(b, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device), "SM count");
     if (resident <= 0) return bfail(b, FC_LBM_ERR_CUDA, "batch kernel occupancy query failed");
-    b->grid = sms * resident * b->mult;
+    b->grid = sms * resident * b->mult;  // 0: one block per work item
     FB_TRY(b, cudaMemcpyAsync(b->d_lat, b->h_lat.data(), b->h_lat.size() * sizeof(fc::BatchLattice),
                               cudaMemcpyHostToDevice, b->stream),
            "upload batch descriptors");
@@ -1523,6 +1555,9 @@ int batch_bulk_members(fc_lbm_batch* b, int parity) {
 int batch_step_direct(fc_lbm_batch* b, int parity) {
     if (b->rows == 0)
         FC_RC(batch_bulk_members(b, parity));
+    else if (b->mult == 0)
+        for (const fc::TileLaunch& t : b->tiles[parity])
+            FB_TRY(b, fc::launch_bulk_tiles(b->q, b->storage, t, b->stream), "batch bulk step");
     else
         FB_TRY(b, fc::launch_bulk_batch(b->q, b->storage, b->rows, b->d_lat, (int)b->m.size(), b->total, parity,
                                         b->grid, b->stream),
@@ -1693,8 +1728,9 @@ int fc_lbm_batch_step(fc_lbm_batch* b, int32_t n) {
 
 int fc_lbm_batch_config(fc_lbm_batch* b, int32_t rows, int32_t grid_mult) {
     if (!b) return FC_LBM_ERR_INVALID_ARG;
-    if ((rows != 0 && rows != 4 && rows != 8 && rows != 16) || (grid_mult != 1 && grid_mult != 2))
-        return bfail(b, FC_LBM_ERR_INVALID_ARG, "rows must be 0, 4, 8 or 16 and grid_mult 1 or 2");
+    if ((rows != 0 && rows != 4 && rows != 8 && rows != 16) || grid_mult < 0 || grid_mult > 2 ||
+        (grid_mult == 0 && rows != 8))
+        return bfail(b, FC_LBM_ERR_INVALID_ARG, "rows must be 0, 4, 8 or 16 and grid_mult 1 or 2 (or 0 with rows 8)");
     b->rows = rows;
     b->mult = grid_mult;
     return FC_LBM_OK;

@@ -164,6 +164,31 @@ struct BatchLattice {
 // rows is 4, 8 or 16.
 cudaError_t launch_bulk_batch(int q, int storage, int rows, const BatchLattice* lat, int nlat,
                               unsigned long long total, int parity, int grid, cudaStream_t s);
+// One lattice of a one-block-per-tile batch launch (k_bulk_pairs_tiles) for
+// one step: its k_bulk_pairs parameters, passed by value with the launch.
+struct TileLattice {
+    Geom g;
+    StepParams p;
+    PlanePtrs pp;
+    const void* fin;
+    void* fout;
+    const uint32_t* bits;
+    int* diverged;
+    unsigned first;  // the launch's first block that is this lattice's
+    int gx, gy;      // x chunks per row, 8-row blocks per layer
+};
+// Lattices per launch: the parameters stay under the 32 KB kernel-parameter
+// limit.
+constexpr int kTileLaunchLattices = 32;
+struct TileLaunch {
+    TileLattice l[kTileLaunchLattices];
+    int nlat;
+    unsigned tiles;  // blocks of the launch
+};
+// The bulk step of up to kTileLaunchLattices lattices of a batch as one block
+// per tile of 64 x 8 cells: block w steps tile w - first of the last lattice
+// whose first <= w.
+cudaError_t launch_bulk_tiles(int q, int storage, const TileLaunch& t, cudaStream_t s);
 // The boundary-list entries of every lattice of a batch in one launch
 // (`total` = the sum of the lattices' list lengths).
 cudaError_t launch_boundary_batch(int q, int storage, const BatchLattice* lat, int nlat, unsigned long long total,

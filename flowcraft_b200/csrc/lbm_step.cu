@@ -151,39 +151,6 @@ __device__ __forceinline__ void plane_cell(const typename S::T* __restrict__ fin
 // holds this lane's bits (1: cell x, 2: cell x + 1). (The FP32 kernels keep
 // plane_cell: there the warp-wide version costs more registers than the
 // kernel has to spare.)
-template <int Q>
-__device__ __forceinline__ float lattice_w_rt(unsigned i) {
-    return i == 0 ? Lattice<Q>::w(0) : (i < 7 ? Lattice<Q>::w(1) : Lattice<Q>::w(Q - 1));
-}
-
-// Component `axis` of e_i for a run-time direction: the table packed two bits
-// per direction (component + 1) into one compile-time constant.
-template <int Q>
-__host__ __device__ constexpr unsigned long long lattice_e_bits(int axis) {
-    unsigned long long b = 0;
-    for (int i = 0; i < Q; ++i) {
-        const int e = axis == 0 ? Lattice<Q>::ex(i) : (axis == 1 ? Lattice<Q>::ey(i) : Lattice<Q>::ez(i));
-        b |= (unsigned long long)(e + 1) << (2 * i);
-    }
-    return b;
-}
-
-template <int Q, int Axis>
-__device__ __forceinline__ float lattice_e_rt(unsigned i) {
-    constexpr unsigned long long bits = lattice_e_bits<Q>(Axis);
-    return (float)((int)((bits >> (2 * i)) & 3ull) - 1);
-}
-
-// equilibrium<Q, I> for a run-time direction: e.u as ((ex ux + ey uy) + ez uz)
-// with e in {-1, 0, 1}, which equals edotu's sum of the non-zero terms (a
-// zero term adds +-0, and only the sign of a zero result can differ, which
-// the equilibrium does not see), then the same operations.
-template <int Q>
-__device__ __forceinline__ float equilibrium_rt(unsigned i, float rho, float ux, float uy, float uz, float u2) {
-    const float eu = (lattice_e_rt<Q, 0>(i) * ux + lattice_e_rt<Q, 1>(i) * uy) + lattice_e_rt<Q, 2>(i) * uz;
-    return (lattice_w_rt<Q>(i) * rho) * (((1.0f + 3.0f * eu) + (4.5f * eu) * eu) - 1.5f * u2);
-}
-
 template <int Q, class S>
 __device__ __forceinline__ void row_end_cell(const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
                                              const Geom& g, const StepParams& p, int px, size_t pc) {
@@ -308,16 +275,17 @@ __device__ __forceinline__ void shell_item(const PairsShell& sh, int& bx, int& b
     }
 }
 
+// One block of k_bulk_pairs: the 64 x kBulkRows cells of x chunk bx, row
+// block by, layer z. shell: the launch covers the shell only (interior warps
+// leave). k_bulk_pairs_tiles runs the same code for the tiles of many
+// lattices in one launch.
 template <int Q, class S>
-__global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs(const typename S::T* __restrict__ fin,
-                                                                typename S::T* __restrict__ fout,
-                                                                const uint32_t* __restrict__ bulk_bits, Geom g,
-                                                                StepParams p, PlanePtrs pp, int z0,
-                                                                int* __restrict__ diverged, PairsShell sh) {
+__device__ __forceinline__ void pairs_tile(const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
+                                           const uint32_t* __restrict__ bulk_bits, const Geom& g,
+                                           const StepParams& p, const PlanePtrs& pp, int* __restrict__ diverged,
+                                           int bx, int by, int z, bool shell) {
     using L = Lattice<Q>;
     using T = typename S::T;
-    int bx = blockIdx.x, by = blockIdx.y, z = z0 + blockIdx.z;
-    if (sh.n) shell_item(sh, bx, by, z);
     const int y = by * kBulkRows + threadIdx.y;
     if (y >= g.ny) return;
     const size_t row = (size_t)z * g.ny + y;
@@ -343,7 +311,7 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs(const typename
     if (!(pair | plane)) return;
     const bool face = (y == 0) | (y == g.ny - 1) | (z == 0) | (z == g.nz - 1);
     const bool edge = (bx == 0) | (64 * bx + 64 >= g.nx);
-    if (sh.n && !face && !edge) return;  // an interior warp: done by k_bulk_tiles
+    if (shell && !face && !edge) return;  // an interior warp: done by k_bulk_tiles
 
     // FP32: the one lane of a row end that holds an inlet or outlet cell finishes it alone
     if (plane) plane_cell<Q, S>(fin, fout, g, p, plane == 1u ? x : x + 1, plane == 1u ? c : (size_t)c + 1);
@@ -397,6 +365,43 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs(const typename
     const unsigned bad = collide_pair<Q, S>(v, p.tau, p.cs) & pair;
     if (bad) atomicOr(diverged, 1);
     store_pair<Q, S>(pp, c, v, pair);
+}
+
+template <int Q, class S>
+__global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs(const typename S::T* __restrict__ fin,
+                                                                typename S::T* __restrict__ fout,
+                                                                const uint32_t* __restrict__ bulk_bits, Geom g,
+                                                                StepParams p, PlanePtrs pp, int z0,
+                                                                int* __restrict__ diverged, PairsShell sh) {
+    int bx = blockIdx.x, by = blockIdx.y, z = z0 + blockIdx.z;
+    if (sh.n) shell_item(sh, bx, by, z);
+    pairs_tile<Q, S>(fin, fout, bulk_bits, g, p, pp, diverged, bx, by, z, sh.n != 0);
+}
+
+// The bulk step of many lattices in one launch of one block per tile: the
+// blocks of each lattice's own k_bulk_pairs launch, in its order, the
+// lattices one after another, so they follow each other through the GPU with
+// no launch boundary between them. Every lattice's k_bulk_pairs parameters
+// travel in this launch's parameters (constant bank): a block finds its
+// lattice by a binary search there and runs k_bulk_pairs' per-tile code, so
+// a batch step is bit-identical to stepping each lattice alone.
+template <int Q, class S>
+__global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_tiles(const __grid_constant__ TileLaunch t) {
+    using T = typename S::T;
+    const unsigned w = blockIdx.x;
+    int lo = 0, hi = t.nlat - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (t.l[mid].first <= w) lo = mid;
+        else hi = mid - 1;
+    }
+    const TileLattice& d = t.l[lo];
+    const unsigned local = w - d.first;
+    const unsigned gx = (unsigned)d.gx, gy = (unsigned)d.gy;
+    const unsigned r = local / gx;
+    const unsigned z = r / gy;
+    pairs_tile<Q, S>(static_cast<const T*>(d.fin), static_cast<T*>(d.fout), d.bits, d.g, d.p, d.pp, d.diverged,
+                     (int)(local - r * gx), (int)(r - z * gy), (int)z, false);
 }
 
 // k_bulk_pairs with the learned closure (16-bit offset storage). The MLP is a
@@ -1288,6 +1293,18 @@ static cudaError_t bulk_batch_t(int rows, const BatchLattice* lat, int nlat, uns
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();
+}
+
+template <int Q, class S>
+static cudaError_t bulk_tiles_t(const TileLaunch& t, cudaStream_t s) {
+    if (t.tiles == 0) return cudaSuccess;
+    if (t.nlat < 1 || t.nlat > kTileLaunchLattices || t.tiles > 0x7fffffffu) return cudaErrorInvalidValue;
+    k_bulk_pairs_tiles<Q, S><<<t.tiles, dim3(32, kBulkRows), 0, s>>>(t);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bulk_tiles(int q, int storage, const TileLaunch& t, cudaStream_t s) {
+    FC_DISPATCH(q, storage, bulk_tiles_t, t, s);
 }
 
 template <int Q, class S>

@@ -148,6 +148,54 @@ __device__ __forceinline__ void aa_plane_cell(typename S::T* f, const Geom& g, c
     });
 }
 
+// aa_plane_cell for the 16-bit formats by the whole warp: lane i < Q takes
+// population i of the cell (the equilibrium for its run-time direction and
+// its slot), so the cell's Q stores are one instruction for the warp. The
+// values are aa_plane_cell's. Every lane of the warp calls aa_row_end_cells
+// together; `plane` holds this lane's bits (1: cell x, 2: cell x + 1).
+template <int Q, class S, bool Odd>
+__device__ __forceinline__ void aa_row_end_cell(typename S::T* f, const Geom& g, const StepParams& p,
+                                                const AaSide& sd, int px, int y, int z, uint32_t pc, size_t row) {
+    const unsigned lane = threadIdx.x & 31;
+    const bool mine = lane < (unsigned)Q;
+    const unsigned i = mine ? lane : 0u;
+    float v;
+    if (px == p.inlet_x) {
+        const float ux = p.inlet_ux;
+        v = equilibrium_rt<Q>(i, 1.0f, ux, 0.0f, 0.0f, speed2(ux, 0.0f, 0.0f));
+    } else {
+        const float4 m = sd.outm[outm_index(sd, Odd ? 1 : 0, p.reverse ? 0 : 1, row)];
+        const float rho = m.x > 1e-6f ? 1.0f + 0.999f * (m.x - 1.0f) : 1.0f;
+        v = equilibrium_rt<Q>(i, rho, m.y, m.z, m.w, speed2(m.y, m.z, m.w));
+    }
+    // the slot out_slot<Q, i, Odd> names, for the run-time direction
+    const unsigned opp = i == 0 ? 0u : ((i - 1u) ^ 1u) + 1u;
+    size_t slot = (size_t)opp * g.n + pc;
+    if constexpr (Odd) {
+        const int ex = (int)lattice_e_rt<Q, 0>(i), ey = (int)lattice_e_rt<Q, 1>(i), ez = (int)lattice_e_rt<Q, 2>(i);
+        const int tx = px + ex, ty = y + ey, tz = z + ez;
+        if (tx >= 0 && ty >= 0 && tz >= 0 && tx < g.nx && ty < g.ny && tz < g.nz)
+            slot = (size_t)i * g.n + (size_t)((long long)pc + ex + (long long)ey * g.nx + (long long)ez * g.nxy);
+    }
+    if (mine) f[slot] = S::enc(v, lattice_w_rt<Q>(i));
+}
+
+template <int Q, class S, bool Odd>
+__device__ __forceinline__ void aa_row_end_cells(typename S::T* f, const Geom& g, const StepParams& p,
+                                                 const AaSide& sd, unsigned plane, int x, int y, int z, uint32_t c,
+                                                 size_t row) {
+    unsigned m = __ballot_sync(0xffffffffu, plane != 0u);
+    while (m) {  // uniform: at most the two row ends
+        const int src = __ffs(m) - 1;
+        m &= m - 1u;
+        const unsigned sp = __shfl_sync(0xffffffffu, plane, src);
+        const int sx = __shfl_sync(0xffffffffu, x, src);
+        const uint32_t sc = __shfl_sync(0xffffffffu, c, src);
+        if (sp & 1u) aa_row_end_cell<Q, S, Odd>(f, g, p, sd, sx, y, z, sc, row);
+        if (sp & 2u) aa_row_end_cell<Q, S, Odd>(f, g, p, sd, sx + 1, y, z, sc + 1u, row);
+    }
+}
+
 }  // namespace
 
 // Bulk cells (bulk mask) of lattices with even nx; see the file comment.
@@ -177,8 +225,12 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_aa(typename S:
         plane |= pair & 2u;
         pair &= ~2u;
     }
-    if (!(pair | plane)) return;
     const uint32_t c = (uint32_t)(row * g.nx + x);
+    if constexpr (!S::kExact) {  // the row-end cells by the whole warp
+        aa_row_end_cells<Q, S, Odd>(f, g, p, sd, plane, x, y, z, c, row);
+        plane = 0;
+    }
+    if (!(pair | plane)) return;
     const bool face = (y == 0) | (y == g.ny - 1) | (z == 0) | (z == g.nz - 1);
     const bool edge = (blockIdx.x == 0) | (64 * (int)blockIdx.x + 64 >= g.nx);
 
@@ -231,17 +283,19 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_aa(typename S:
                     dst[c + 1u] = h.y;
                 }
             });
-        } else {  // a partial pair of a row-end warp: its valid cell only
+        } else {  // a partial pair of a row-end warp: its valid cell only (pair is 1 or 2)
+            const uint32_t ec = pair == 1u ? c : c + 1u;
             static_for<0, Q>([&](auto I) {
                 constexpr int i = decltype(I)::value;
-                T* dst = static_cast<T*>(pp.dst[i]) + c;
-                T2 h;
-                if constexpr (S::kExact)
-                    h = S::enc2(v[i].x, v[i].y, L::w(i));
-                else
-                    h = S::pack2(v[i].x, v[i].y);
-                if (pair & 1u) dst[0] = h.x;
-                if (pair & 2u) dst[1] = h.y;
+                if constexpr (S::kExact) {
+                    const T2 h = S::enc2(v[i].x, v[i].y, L::w(i));
+                    T* dst = static_cast<T*>(pp.dst[i]) + c;
+                    if (pair & 1u) dst[0] = h.x;
+                    if (pair & 2u) dst[1] = h.y;
+                } else {
+                    const T2 h = S::pack2(v[i].x, v[i].y);
+                    static_cast<T*>(pp.dst[i])[ec] = pair == 1u ? h.x : h.y;
+                }
             });
         }
         if (edge) {  // upstream-neighbour moments for the outlets of both flow directions
@@ -491,13 +545,10 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_aa_learned(typ
     const bool face = (y == 0) | (y == g.ny - 1) | (z == 0) | (z == g.nz - 1);
     // off the faces every source slot lies inside the set (k_bulk_pairs_aa)
     const bool fast = !face;
+    aa_row_end_cells<Q, S, Odd>(f, g, p, sd, plane, x, y, z, c, row);
 
     float2 v[Q];
     if (fast) {
-        if (plane) {
-            const int px = plane == 1u ? x : x + 1;
-            aa_plane_cell<Q, S, Odd>(f, g, p, sd, px, y, z, plane == 1u ? c : c + 1u, row);
-        }
         static_for<0, Q>([&](auto I) {
             constexpr int i = decltype(I)::value;
             const T* src = static_cast<const T*>(pp.src[i]);
@@ -507,10 +558,6 @@ __global__ void __launch_bounds__(32 * kBulkRows, 4) k_bulk_pairs_aa_learned(typ
                 v[i] = make_float2(S::raw(ld_plain<S>(src + cs)), S::raw(ld_plain<S>(src + cs + 1u)));
         });
     } else {
-        if (plane) {
-            const int px = plane == 1u ? x : x + 1;
-            aa_plane_cell<Q, S, Odd>(f, g, p, sd, px, y, z, plane == 1u ? c : c + 1u, row);
-        }
         const bool va = pair & 1u, vb = pair & 2u;
         static_for<0, Q>([&](auto I) {
             constexpr int i = decltype(I)::value;

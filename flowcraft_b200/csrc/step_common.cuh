@@ -59,6 +59,42 @@ __device__ __forceinline__ unsigned collide_pair(float2 (&v)[Q], float tau, floa
     }
 }
 
+// Lattice constants for a run-time direction i (lane i of a warp that
+// shares one cell's populations): the weight, and each component of e_i from
+// a table packed two bits per direction (component + 1).
+template <int Q>
+__device__ __forceinline__ float lattice_w_rt(unsigned i) {
+    return i == 0 ? Lattice<Q>::w(0) : (i < 7 ? Lattice<Q>::w(1) : Lattice<Q>::w(Q - 1));
+}
+
+// Component `axis` of e_i for a run-time direction: the table packed two bits
+// per direction (component + 1) into one compile-time constant.
+template <int Q>
+__host__ __device__ constexpr unsigned long long lattice_e_bits(int axis) {
+    unsigned long long b = 0;
+    for (int i = 0; i < Q; ++i) {
+        const int e = axis == 0 ? Lattice<Q>::ex(i) : (axis == 1 ? Lattice<Q>::ey(i) : Lattice<Q>::ez(i));
+        b |= (unsigned long long)(e + 1) << (2 * i);
+    }
+    return b;
+}
+
+template <int Q, int Axis>
+__device__ __forceinline__ float lattice_e_rt(unsigned i) {
+    constexpr unsigned long long bits = lattice_e_bits<Q>(Axis);
+    return (float)((int)((bits >> (2 * i)) & 3ull) - 1);
+}
+
+// equilibrium<Q, I> for a run-time direction: e.u as ((ex ux + ey uy) + ez uz)
+// with e in {-1, 0, 1}, which equals edotu's sum of the non-zero terms (a
+// zero term adds +-0, and only the sign of a zero result can differ, which
+// the equilibrium does not see), then the same operations.
+template <int Q>
+__device__ __forceinline__ float equilibrium_rt(unsigned i, float rho, float ux, float uy, float uz, float u2) {
+    const float eu = (lattice_e_rt<Q, 0>(i) * ux + lattice_e_rt<Q, 1>(i) * uy) + lattice_e_rt<Q, 2>(i) * uz;
+    return (lattice_w_rt<Q>(i) * rho) * (((1.0f + 3.0f * eu) + (4.5f * eu) * eu) - 1.5f * u2);
+}
+
 // Storage code of a format (0 FP32, 1 FP16 offset, 2 BF16 offset).
 template <class S>
 constexpr int storage_code() {

@@ -422,23 +422,28 @@ FC_LBM_API int fc_lbm_particles_set(fc_lbm* h, const float* points, size_t point
  * their own state and API; they must outlive the batch and must not step on
  * their own while a batch step is queued. */
 typedef struct fc_lbm_batch fc_lbm_batch;
-#define FC_LBM_BATCH_CANDIDATES 7
+#define FC_LBM_BATCH_CANDIDATES 8
 FC_LBM_API int fc_lbm_batch_create(fc_lbm* const* members, int32_t count, fc_lbm_batch** out);
 FC_LBM_API void fc_lbm_batch_destroy(fc_lbm_batch* b);
 FC_LBM_API const char* fc_lbm_batch_last_error(const fc_lbm_batch* b);
 /* n steps of every member; asynchronous, ordered after and before the
  * members' own streams. An odd n leaves the next call to rebuild its graph. */
 FC_LBM_API int fc_lbm_batch_step(fc_lbm_batch* b, int32_t n);
-/* The block shape of the persistent launch: rows in {4, 8, 16} (a block is 32
- * x rows threads over 64 x rows cells), grid_mult in {1, 2} (resident blocks
- * per SM times this). rows 0 replaces the persistent launch by each member's
- * own bulk kernel (the one fc_lbm_step launches), spread over 4 forked
- * streams; grid_mult is then unused. Default 8, 1. */
+/* The block shape of the batch's bulk launch: rows in {4, 8, 16} (a block is
+ * 32 x rows threads over 64 x rows cells) with grid_mult in {1, 2} (a
+ * persistent launch of resident blocks per SM times this, each block taking
+ * chunks of 8 tiles), or rows 8 with grid_mult 0 (one block per tile over the
+ * tiles of every lattice, each lattice's in the order of its own launch, the
+ * lattices one after another; one launch per 32 lattices). rows 0
+ * replaces the batch launch by each member's own bulk kernel (the one
+ * fc_lbm_step launches), spread over 4 forked streams; grid_mult is then
+ * unused. Default 8, 1. */
 FC_LBM_API int fc_lbm_batch_config(fc_lbm_batch* b, int32_t rows, int32_t grid_mult);
 /* Autotuner: times each of the FC_LBM_BATCH_CANDIDATES shapes (rows 4, 8, 16
- * x grid_mult 1, 2, in that order, then rows 0) over `steps` (rounded up to
- * even) real steps after 2 warm-up steps, and keeps the fastest. Every member
- * advances by 7 x (steps + 2) steps (the candidates compute identical results).
+ * x grid_mult 1, 2, in that order, then rows 8 with grid_mult 0, then rows 0)
+ * over `steps` (rounded up to even) real steps after 2 warm-up steps, and
+ * keeps the fastest. Every member advances by 8 x (steps + 2) steps (the
+ * candidates compute identical results).
  * ms_per_step (may be NULL) receives each candidate's time. Blocking. */
 FC_LBM_API int fc_lbm_batch_tune(fc_lbm_batch* b, int32_t steps, int32_t* rows, int32_t* grid_mult,
                                  float* ms_per_step);

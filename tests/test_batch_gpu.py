@@ -1,6 +1,7 @@
 """Batches (fc_lbm_batch_*): many lattices of uneven sizes stepped by one
-persistent launch per step, with CUDA-graph replay and the autotuner, must
-give the same bits as stepping every lattice on its own."""
+bulk launch per step (persistent, or one block per tile) or by the members'
+own bulk kernels side by side, with CUDA-graph replay and the autotuner,
+must give the same bits as stepping every lattice on its own."""
 import numpy as np
 import pytest
 
@@ -45,7 +46,7 @@ def test_batch_is_bit_identical_to_single_steps(gpu, storage, q):
     for s in single:
         s.Step(None, 17)
     _same(batched, single)
-    for rows, mult in ((4, 2), (16, 1), (0, 1)):
+    for rows, mult in ((4, 2), (16, 1), (8, 0), (0, 1)):
         b.Config(rows, mult)
         b.Step(4)
         for s in single:
@@ -85,8 +86,8 @@ def test_blocks_that_take_many_chunks(gpu):
     batched, single = make(), make()
     assert sum(s.CellCount() for s in batched) > 6_000_000
     b = LbmBatch(batched)
-    for rows in (16, 4):
-        b.Config(rows, 1)
+    for rows, mult in ((16, 1), (4, 1), (8, 0)):
+        b.Config(rows, mult)
         b.Step(4)
         for s in single:
             s.Step(None, 4)
@@ -98,14 +99,14 @@ def test_blocks_that_take_many_chunks(gpu):
 
 
 def test_tuner_picks_a_shape_and_keeps_results(gpu):
-    from flowcraft_b200.batch import LbmBatch
+    from flowcraft_b200.batch import CANDIDATES, LbmBatch
     batched, single = _make("FP16_OFFSET"), _make("FP16_OFFSET")
     b = LbmBatch(batched)
     r = b.Tune(steps=4)
-    assert (r["rows"], r["grid_mult"]) in [(4, 1), (4, 2), (8, 1), (8, 2), (16, 1), (16, 2), (0, 1)]
-    assert len(r["ms_per_step"]) == 7 and all(v > 0 for v in r["ms_per_step"].values())
+    assert (r["rows"], r["grid_mult"]) in CANDIDATES
+    assert len(r["ms_per_step"]) == len(CANDIDATES) == 8 and all(v > 0 for v in r["ms_per_step"].values())
     for s in single:
-        s.Step(None, 7 * (4 + 2))
+        s.Step(None, len(CANDIDATES) * (4 + 2))
     b.Step(8)
     for s in single:
         s.Step(None, 8)

@@ -64,7 +64,8 @@ def test_committed_traffic_figures_are_read():
 
 def test_batch_shape_option_and_candidate_table():
     """--batch-shape parses, and the Python candidate list matches the C
-    header's count and the library's table (persistent shapes, then rows 0)."""
+    header's count and the library's table (persistent shapes, one block per
+    tile, then rows 0)."""
     import re
     from flowcraft_b200.batch import CANDIDATES
     assert bench.parse_args(["--batch-shape", "0x1"]).batch_shape == "0x1"
@@ -73,6 +74,6 @@ def test_batch_shape_option_and_candidate_table():
     n = int(re.search(r"#define FC_LBM_BATCH_CANDIDATES (\d+)", hdr).group(1))
     assert len(CANDIDATES) == n
     src = open(os.path.join(ROOT, "flowcraft_b200", "csrc", "fc_lbm.cu")).read()
-    table = re.search(r"kBatchCand\[FC_LBM_BATCH_CANDIDATES\]\[2\] = \{(.*?)\};", src).group(1)
+    table = re.search(r"kBatchCand\[FC_LBM_BATCH_CANDIDATES\]\[2\] = \{(.*?)\};", src, re.S).group(1)
     pairs = [tuple(int(v) for v in m) for m in re.findall(r"\{(\d+), (\d+)\}", table)]
     assert pairs == CANDIDATES
