@@ -98,6 +98,42 @@ def test_blocks_that_take_many_chunks(gpu):
         s.close()
 
 
+def test_one_block_per_tile_over_many_lattices(gpu):
+    """40 small lattices of varied sizes and parameters: the one-block-per-tile
+    form carries at most 32 lattices in one launch's parameters, so a step
+    takes two launches; every lattice keeps the bits of single stepping."""
+    from flowcraft_b200.batch import LbmBatch
+    from flowcraft_b200.lbm import LatticeModel, LbmSolver, Params, Storage, VoxelGrid
+
+    def make():
+        out = []
+        r = np.random.default_rng(7)
+        for k in range(40):
+            nx = int(r.integers(8, 33)) * 2
+            ny, nz = int(r.integers(8, 25)), int(r.integers(8, 25))
+            solid, sdf = geometry({"kind": "sphere", "dims": [nx, ny, nz],
+                                   "center": [nx / 3.0, ny / 2.0, nz / 2.0], "r": min(ny, nz) / 5.0})
+            s = LbmSolver()
+            assert s.Init(0, VoxelGrid(nx, ny, nz, solid=solid.ravel(), signedDistance=sdf.ravel()),
+                          LatticeModel.D3Q19, Storage.FP16_OFFSET)
+            s.Reset(Params(tau=float(r.uniform(0.52, 0.6)), inletVelocity=float(r.uniform(0.03, 0.07)),
+                           smagorinskyCs=0.1, reverseFlow=bool(k % 5 == 3)), True)
+            out.append(s)
+        return out
+
+    batched, single = make(), make()
+    b = LbmBatch(batched)
+    b.Config(8, 0)
+    b.Step(7)  # three graph replays of two launches per step, then one direct step
+    for s in single:
+        s.Step(None, 7)
+    _same(batched, single)
+    assert not any(s.HasDiverged() for s in batched)
+    b.close()
+    for s in batched + single:
+        s.close()
+
+
 def test_tuner_picks_a_shape_and_keeps_results(gpu):
     from flowcraft_b200.batch import CANDIDATES, LbmBatch
     batched, single = _make("FP16_OFFSET"), _make("FP16_OFFSET")
