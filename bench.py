@@ -283,6 +283,23 @@ def spinup_of(args, variant) -> int:
     return args.spinup if variant.endswith("_learned") else 0
 
 
+def workload_config(args, cfg, world) -> dict:
+    """The `config` of the bench line: the workload and the headline variant's
+    formats, the same for both arms (no run-dependent values)."""
+    head = [v.strip() for v in args.variants.split(",") if v.strip()][0]
+    learned = head.endswith("_learned")
+    spin = spinup_of(args, head)
+    return {"workload": cfg["desc"], "lattice": "D3Q19", "nx": cfg["nx"], "ny": cfg["ny"], "nz": cfg["nz"],
+            "cells": cfg["nx"] * cfg["ny"] * cfg["nz"], "storage": head, "collision": "regularized, FP32",
+            "closure": ("learned 5-32-32-1 MLP per cell (BF16 mma.sync, FP32 accumulate), Smagorinsky "
+                        f"Cs={cfg['cs']} outside its range; data/closure_c4.json" if learned else "Smagorinsky"),
+            "streaming": "AA pattern, one set in place" if "_aa" in head else "pull, ping-pong",
+            "flow_state": (f"timed after {spin} + {args.warmup} steps from the mid-speed seed" if spin
+                           else f"timed after {args.warmup} steps from the seed"),
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "l2": "no flush: populations 10.2 GB (fp16) / 20.4 GB (fp32) per copy, L2 126 MB"}
+
+
 def kernel_of(variant) -> str:
     name = ("k_bulk_pairs" + ("_aa" if "_aa" in variant else "") + ("_learned" if variant.endswith("_learned") else "")
             + ("_tc" if "_tc_" in variant else ""))
@@ -383,8 +400,9 @@ def run_reference_arm(args, cfg, rank, world):
         "impl": "reference", "metric": METRIC, "value": r["glups"], "unit": "GLUPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": cfg["desc"], "lattice": "D3Q19", "sample_cells": r["cells"]},
-        "cpu_baseline": {"value": r["glups"], "unit": "GLUPS", "cores": cores, "kind": r["kind"], "sample": sample},
+        "config": workload_config(args, cfg, world),
+        "cpu_baseline": {"value": r["glups"], "unit": "GLUPS", "cores": cores, "kind": r["kind"], "sample": sample,
+                         "sample_cells": r["cells"]},
         "e2e": {"value": r["glups"], "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -466,12 +484,11 @@ def run_e2e(args, cfg, solid, sdf, variant, dev_index):
     s.close()
     h2d = n * (1 + 4)
     d2h = 4 * steps + n * 16 + 96  # the probe's verdict flag per step, the stats, the field
-    return {"value": n * steps / el / 1e9, "unit": "GLUPS", "seconds": el, "steps": steps,
+    return {"value": round(n * steps / el / 1e9, 3), "unit": "GLUPS", "seconds": round(el, 3), "steps": steps,
             "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps,
-            "diverged": diverged, "avg_density": stats.avgDensity,
-            "timed": "Init(host VoxelGrid) + Reset + SetClosure (learned variants) + steps x (Step(1) + "
-                     "ProbeSliceHealth) + ReadbackStats + ReadbackFieldRange(all z); steps = spin-up + timed "
-                     "steps for the learned variants"}
+            "diverged": diverged, "avg_density": round(stats.avgDensity, 6),
+            "timed": "Init(host grid)+Reset+SetClosure+steps*(Step(1)+ProbeSliceHealth)+ReadbackStats+"
+                     "ReadbackFieldRange(all z); steps include the learned variants' spin-up"}
 
 
 def time_batch(args, cfg, local_rank, dist_on, steps, sample_clocks):
@@ -666,9 +683,9 @@ def run_ours(args, cfg, rank, world, local_rank):
     peak, peak_src = measured_peak()
     trf = ncu_traffic_per_cell(head["variant"], developed=head["spinup_steps"] > 0)
     roofline = {
-        "bound": "hbm", "achieved": head["bulk_gbs"], "peak": peak, "unit": "GB/s",
-        "frac": head["bulk_gbs"] / peak if head["bulk_gbs"] else None,
-        "traffic": trf * head["bulk_cells"] if trf else None,
+        "bound": "hbm", "achieved": round(head["bulk_gbs"], 1) if head["bulk_gbs"] else None, "peak": peak,
+        "unit": "GB/s", "frac": round(head["bulk_gbs"] / peak, 4) if head["bulk_gbs"] else None,
+        "traffic": int(trf * head["bulk_cells"]) if trf else None,
         "kernel": kernel_of(head["variant"]) + " (all bulk-mask cells)",
         "algorithmic_bytes_per_launch": head["bulk_bytes_per_launch"],
         "peak_source": ("measured: MEASURED_PEAKS.json hbm_gbs" if peak_src == "measured"
@@ -699,8 +716,8 @@ def run_ours(args, cfg, rank, world, local_rank):
         s_np, d_np, z0 = cpu_subbox(cfg, solid, sdf, cores)
         r = run_cpu_reference(cfg, s_np, d_np, 10 ** 6, 1, seconds=args.cpu_seconds)
         cpu = {"value": r["glups"], "unit": "GLUPS", "cores": cores, "kind": r["kind"],
-               "sample": f"LbmReference::Step on a z-truncated {cfg['nx']}x{cfg['ny']}x{s_np.shape[0]} sub-box "
-                         f"(z0={z0}) of the same lattice, {r['steps']} steps in {r['seconds']:.1f}s after 1 warm-up"}
+               "sample": f"LbmReference::Step, {cfg['nx']}x{cfg['ny']}x{s_np.shape[0]} sub-box (z0={z0}) of the "
+                         f"lattice, {r['steps']} steps in {r['seconds']:.1f}s after 1 warm-up"}
     if rank != 0:
         return 0
     variants_out = {}
@@ -721,18 +738,11 @@ def run_ours(args, cfg, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: procedural aircraft mesh voxelized on the device, no dataset",
-        "config": {"workload": cfg["desc"], "lattice": "D3Q19", "nx": cfg["nx"], "ny": cfg["ny"], "nz": cfg["nz"],
-                   "cells": cells, "storage": head["variant"], "collision": "regularized, FP32",
-                   "closure": ("learned MLP 5-32-32-1 (BF16 tensor-core MMA, FP32 accumulate) per cell, Smagorinsky "
-                               "Cs=0.1 outside its training range; weights flowcraft_b200/data/closure_c4.json"
-                               if head["variant"].endswith("_learned") else "Smagorinsky"),
-                   "streaming": "AA pattern, one set in place" if "_aa" in head["variant"] else "pull, ping-pong",
-                   "flow_state": (f"timed after {head['spinup_steps']} + {args.warmup} steps from the mid-speed seed"
-                                  if head["spinup_steps"] else f"timed after {args.warmup} steps from the seed"),
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": "no flush: the population set (10.2 GB fp16 / 20.4 GB fp32 per copy) exceeds the 126 MB L2",
-                   "boundary_cells": head["boundary_cells"], "bouzidi_links": head["bouzidi_links"],
-                   "closure_coverage": head["closure_coverage"]},
+        "config": workload_config(args, cfg, world),
+        "lattice_run": {"boundary_cells": head["boundary_cells"], "bouzidi_links": head["bouzidi_links"],
+                        "closure_coverage": ({"cell_fraction": round(head["closure_coverage"]["cell_fraction"], 4),
+                                              "warp_fraction": round(head["closure_coverage"]["warp_fraction"], 4)}
+                                             if head["closure_coverage"] else None)},
         "variants": variants_out,
         "batch_c3": batch_c3,
         "roofline": roofline,
@@ -741,7 +751,7 @@ def run_ours(args, cfg, rank, world, local_rank):
         "gpu_launches": head["launches"],
         "clocks": head["clocks"],
     }
-    print(json.dumps(line), flush=True)
+    print(json.dumps(line, separators=(",", ":")), flush=True)
     return 0
 
 

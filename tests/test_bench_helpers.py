@@ -77,3 +77,17 @@ def test_batch_shape_option_and_candidate_table():
     table = re.search(r"kBatchCand\[FC_LBM_BATCH_CANDIDATES\]\[2\] = \{(.*?)\};", src, re.S).group(1)
     pairs = [tuple(int(v) for v in m) for m in re.findall(r"\{(\d+), (\d+)\}", table)]
     assert pairs == CANDIDATES
+
+
+def test_both_arms_share_the_workload_config():
+    """The reference arm prints the same `config` as this arm's line (the
+    driver compares them); run-dependent values stay out of it."""
+    import inspect
+    args = bench.parse_args([])
+    cfg = bench.CONFIGS["large"]
+    c = bench.workload_config(args, cfg, 1)
+    assert c == bench.workload_config(args, cfg, 1)
+    assert c["storage"] == args.variants.split(",")[0] and c["cells"] == cfg["nx"] * cfg["ny"] * cfg["nz"]
+    assert not {"boundary_cells", "bouzidi_links", "closure_coverage", "sample_cells"} & set(c)
+    for arm in (bench.run_reference_arm, bench.run_ours):
+        assert "workload_config(args, cfg, world)" in inspect.getsource(arm)
