@@ -87,6 +87,10 @@ BRANCHES = {
     "wide_q15": _sphere((160, 40, 40), (52, 20, 20), 7, 15, tau=0.56, inlet_velocity=0.06, smagorinsky_cs=0.1),
     "wide_nosdf": dict(_sphere((128, 34, 30), (40, 17, 15), 6.5, 19, free_slip_z=0), geom={
         "kind": "sphere", "dims": [128, 34, 30], "center": [40, 17, 15], "r": 6.5, "sdf": False}),
+    # four 64-cell chunks per row with the sphere in the second: warps off the
+    # row ends hold pairs cut by the wall (one cell bulk, one wall-adjacent)
+    "interior_chunks": _sphere((256, 22, 20), (101.5, 11, 10), 5.3, 19, tau=0.57, inlet_velocity=0.06,
+                               smagorinsky_cs=0.1),
 }
 
 
