@@ -1,7 +1,7 @@
 /*
  * ORACLE — test infrastructure only. Nothing in the product library links,
  * loads or calls this file; only tests/, __graft_entry__.smoke() and
- * bench.py's CPU-baseline leg use it, and only as the checker.
+ * bench.py's CPU-baseline leg use it, and only to check results.
  *
  * A plain-C restatement of FlowCraft's CPU Lattice-Boltzmann step
  * (FlowCraft/LbmReference.cpp) written from the algorithm, compiled twice:
