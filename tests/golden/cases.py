@@ -96,6 +96,14 @@ CASES = {
                      seed_mid=True, steps=[9]),
     "warmstart_q19": dict(geom=SPHERE48, q=19, params=REF_TEST, seed_mid=True, steps=[20, 20],
                           reset_from_field_after=20),
+    # four 64-cell chunks per row with the sphere in the second: pairs cut by
+    # the wall inside a row (the one-cell path of warps off the row ends)
+    "interior_q19": dict(geom={"kind": "sphere", "dims": [256, 22, 20], "center": [101.5, 11, 10], "r": 5.3},
+                         q=19, params=dict(tau=0.57, inlet_velocity=0.06, smagorinsky_cs=0.1), seed_mid=True,
+                         steps=[60]),
+    "interior_q15": dict(geom={"kind": "sphere", "dims": [256, 22, 20], "center": [101.5, 11, 10], "r": 5.3},
+                         q=15, params=dict(tau=0.6, inlet_velocity=0.05, smagorinsky_cs=0.12), seed_mid=True,
+                         steps=[60]),
     # plain-FP32 parity configuration: 128x64x64, sphere r=10 at (40,32,32),
     # U=0.05, Re=100 on the diameter -> nu = 0.05*20/100, tau = 3nu + 1/2
     "c1_q19": dict(geom={"kind": "sphere", "dims": [128, 64, 64], "center": [40, 32, 32], "r": 10}, q=19,
