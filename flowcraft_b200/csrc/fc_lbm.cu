@@ -1527,9 +1527,11 @@ int batch_build(fc_lbm_batch* b) {
 }
 
 // Every member's own bulk kernel (the launch fc_lbm_step makes), spread over
-// the forked streams so that small lattices run side by side; joined back
-// into the batch stream. Under stream capture the fork and join become graph
-// dependencies.
+// the forked streams so that small lattices run side by side, and meanwhile
+// the batch's boundary-list launch on the batch stream (it writes only
+// boundary-list cells and reads only the input sets, so it shares nothing
+// with the bulk kernels); joined back into the batch stream. Under stream
+// capture the fork and join become graph dependencies.
 int batch_bulk_members(fc_lbm_batch* b, int parity) {
     const int nf = (int)std::min<size_t>(fc_lbm_batch::kFork, b->m.size());
     FB_TRY(b, cudaEventRecord(b->ev_fork, b->stream), "fork event");
@@ -1542,6 +1544,8 @@ int batch_bulk_members(fc_lbm_batch* b, int parity) {
         int nl = 0;
         e = launch_bulk(h, step_params(h), h->pop[side], h->pop[1 - side], 0, h->g.nz, b->fork[k % nf], &nl);
     }
+    if (e == cudaSuccess)
+        e = fc::launch_boundary_batch(b->q, b->storage, b->d_lat, (int)b->m.size(), b->btotal, parity, b->stream);
     // always join, so that a capture can end
     for (int j = 0; j < nf; ++j) {
         const cudaError_t r = cudaEventRecord(b->ev_join[j], b->fork[j]);
@@ -1554,8 +1558,8 @@ int batch_bulk_members(fc_lbm_batch* b, int parity) {
 // One step of every member (parity relative to the members' current sets).
 int batch_step_direct(fc_lbm_batch* b, int parity) {
     if (b->rows == 0)
-        FC_RC(batch_bulk_members(b, parity));
-    else if (b->mult == 0)
+        return batch_bulk_members(b, parity);  // the boundary launch runs beside the members' bulk kernels
+    if (b->mult == 0)
         for (const fc::TileLaunch& t : b->tiles[parity])
             FB_TRY(b, fc::launch_bulk_tiles(b->q, b->storage, t, b->stream), "batch bulk step");
     else
