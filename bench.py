@@ -445,11 +445,13 @@ def time_variant(args, cfg, solid, sdf, variant, dev_index, dist_on, sample_cloc
     }
 
 
-def run_e2e(args, cfg, solid, sdf, variant, dev_index):
+def run_e2e(args, cfg, solid, sdf, variant, dev_index, world=1, dist_on=False):
     """The same metric end to end through the public API with host buffers:
     Init from pinned host geometry (H2D), Reset, then per step Step(1) plus
     ProbeSliceHealth of one z-layer (D2H), then ReadbackStats and the full
-    4-float field into host memory (D2H). Wall clock around the host calls.
+    4-float field into host memory (D2H). Wall clock around the host calls,
+    the slowest rank's under torchrun (every rank runs its own lattice), and
+    the value and bytes are the whole job's.
     For the learned variants the spin-up steps are part of the job and of the
     timed region, so the number is the whole run's rate from the seed."""
     import numpy as np
@@ -466,6 +468,7 @@ def run_e2e(args, cfg, solid, sdf, variant, dev_index):
     steps = spinup_of(args, variant) + args.steps
     grid = VoxelGrid(cfg["nx"], cfg["ny"], cfg["nz"], solid=h_solid.numpy(), signedDistance=h_sdf.numpy())
     torch.cuda.synchronize()
+    barrier_sync(dist_on)
     s = LbmSolver()
     t0 = time.perf_counter()
     if not s.Init(dev_index, grid, LatticeModel.D3Q19, st, streaming_of(variant)):
@@ -480,11 +483,11 @@ def run_e2e(args, cfg, solid, sdf, variant, dev_index):
         diverged |= s.ProbeSliceHealth(k % cfg["nz"])
     stats = s.ReadbackStats()
     s.ReadbackFieldRange(0, cfg["nz"], out)
-    el = time.perf_counter() - t0
+    el = allreduce_max(time.perf_counter() - t0, dist_on)
     s.close()
-    h2d = n * (1 + 4)
-    d2h = 4 * steps + n * 16 + 96  # the probe's verdict flag per step, the stats, the field
-    return {"value": round(n * steps / el / 1e9, 3), "unit": "GLUPS", "seconds": round(el, 3), "steps": steps,
+    h2d = world * n * (1 + 4)
+    d2h = world * (4 * steps + n * 16 + 96)  # the probe's verdict flag per step, the stats, the field
+    return {"value": round(world * n * steps / el / 1e9, 3), "unit": "GLUPS", "seconds": round(el, 3), "steps": steps,
             "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps,
             "diverged": diverged, "avg_density": round(stats.avgDensity, 6),
             "timed": "Init(host grid)+Reset+SetClosure+steps*(Step(1)+ProbeSliceHealth)+ReadbackStats+"
@@ -709,7 +712,7 @@ def run_ours(args, cfg, rank, world, local_rank):
     e2e = None
     if not args.no_e2e:
         torch.cuda.empty_cache()
-        e2e = run_e2e(args, cfg, solid, sdf, variants[0], dev_index)
+        e2e = run_e2e(args, cfg, solid, sdf, variants[0], dev_index, world, dist_on)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cores = os.cpu_count() or 1
